@@ -1,0 +1,373 @@
+"""Benchmark of the GLAC hot path on B200.
+
+Workload (one GPU): gradient flow of a 32^3 x 64 lattice (2,097,152 sites) at
+beta = 6.2, links in FP32 with FP64 reductions, Luscher RK3 at eps = 0.01,
+Morningstar-Peardon exponential; the start field is a seeded Haar field after
+600 checkerboard Metropolis sweeps (10 hits, SU3Eps = 0.24).  One "step" is one
+RK3 flow step followed by the plaquette / energy / topological-charge
+measurement, as GLAC's System::flowConfiguration does per flow step.
+
+Metric: flow site-steps/s (sites x steps / s), higher is better.  Also
+reported: the same without per-step observables, FP64, Metropolis
+link-updates/s, the roofline of the flow-stage kernel, the reference's CPU
+path timed on this host, and an end-to-end number through the C ABI with host
+buffers.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank flows its own independent lattice (replicas,
+no collective on the data path); value = all ranks' site-steps / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (32, 32, 32, 64)
+BETA = 6.2
+FLOW_EPS = 0.01
+SU3_EPS = 0.24
+NHITS = 10
+THERM_SWEEPS = 600
+METRIC = "flow site-steps/s at 32^3x64 (RK3 step + plaq/E/Q measurement per step)"
+UNIT = "site-steps/s"
+WORKLOAD = "GLAC gradient flow 32^3x64, beta=6.2, eps=0.01, FP32 links + FP64 sums, per-step observables"
+# algorithmic bytes per site for the three RK3 stages in FP32 (18 reals/link, 8 reals/force):
+# reads 4 links + writes 4 links per stage, force written (stage 0), read+written (1), read (2)
+STAGE_BYTES_FP32 = (8 * 72 + 4 * 32, 8 * 72 + 8 * 32, 8 * 72 + 4 * 32)
+STAGE_BYTES_FP64 = tuple(2 * b for b in STAGE_BYTES_FP32)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference (oracle/_ref) or the oracle port, one process per core
+# ---------------------------------------------------------------------------
+def _cpu_worker(args):
+    kind, dims, nsteps, seed = args
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Oracle, Reference
+    o = Oracle()
+    links = o.haar_field(dims, seed)
+    if kind == "reference":
+        r = Reference()
+        r.configure(dims[0], dims[3], beta=BETA, flow_eps=FLOW_EPS, nflows=nsteps)
+        t0 = time.perf_counter()
+        dt = r.time_flow_measure(links, nsteps)
+        return dt, time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cur = links
+    for _ in range(nsteps):
+        cur = o.flow(dims, cur, FLOW_EPS, 1)
+        o.observables(dims, cur)
+    dt = time.perf_counter() - t0
+    return dt, dt
+
+
+def cpu_kind():
+    from oracle.oracle import REF_SO
+    return "reference" if os.path.exists(REF_SO) else "port"
+
+
+def cpu_flow_rate(nsteps_per_worker: int, dims=(8, 8, 8, 16), workers=None):
+    """Aggregate CPU site-steps/s of flow + per-step observables over all host cores."""
+    kind = cpu_kind()
+    workers = workers or os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    V = int(np.prod(dims))
+    with ctx.Pool(workers) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_cpu_worker, [(kind, dims, nsteps_per_worker, 1000 + i) for i in range(workers)])
+        wall = time.perf_counter() - t0
+    slowest = max(r[0] for r in res)
+    value = workers * V * nsteps_per_worker / slowest
+    sample = (f"{workers} processes x {nsteps_per_worker} steps (RK3 flow + MasterSamplerTopcXYZ) on independent "
+              f"{dims[0]}^3x{dims[3]} Haar fields; {'GLAC sources compiled as oracle/_ref' if kind == 'reference' else 'oracle C port'}")
+    return {"value": value, "unit": UNIT, "cores": workers, "kind": kind, "sample": sample,
+            "wall_s": round(wall, 2), "per_core": value / workers}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args):
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu_base = cpu_flow_rate(args.cpu_steps)  # before the first GPU call (spawned pool)
+
+    import glac_b200 as g
+
+    V = int(np.prod(DIMS))
+    L = g.Lattice(DIMS, beta=BETA, precision="fp32", n_updates=NHITS, su3_eps=SU3_EPS, flow_eps=FLOW_EPS,
+                  seed=20261203, stream_id=rank, reunit_interval=0, device=local)
+    stream = torch.cuda.ExternalStream(L.stream)
+
+    def timed(fn, n):
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        return max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+
+    # start configuration: Haar hot start + 600 Metropolis sweeps (FP32), timed for link-updates/s
+    L.hot_start(20261203)
+    L.metropolis(5)
+    L.reunitarize()
+    acc_holder = {}
+    t_metro = timed(lambda: acc_holder.setdefault("a", L.metropolis(1)), 20)
+    L.metropolis(THERM_SWEEPS - 25)
+    L.reunitarize()
+    start = np.empty((4, V, 18))
+    L.get_links(start)
+    metro_rate = world * 4 * V * 20 / t_metro
+
+    obs_buf = np.empty((args.steps + 1, 3 + DIMS[3]))
+
+    L.flow(args.warmup, measure=True)
+    n0 = L.launch_count
+    clk = ClockSampler(local)
+    clk.start()
+    # timed: K RK3 steps, each followed by the observable measurement (device
+    # buffer), all K+1 observable vectors copied back at the end
+    t_main = timed(lambda: L.flow(args.steps, out=obs_buf), 1)
+    clocks = clk.stop()
+    launches = L.launch_count - n0
+    value = world * V * args.steps / t_main
+
+    t_noobs = timed(lambda: L.flow(args.steps, measure=False), 1)
+    rate_noobs = world * V * args.steps / t_noobs
+
+    # roofline of the flow-stage kernel: CUDA events around each stage launch on
+    # the lattice's stream, averaged over reps RK3 steps
+    reps = max(3, min(args.steps, 20))
+    st = np.array(L.flow_stage_times(reps))
+    hbm_peak, peak_kind = load_peaks()
+    alg_bytes = sum(STAGE_BYTES_FP32) * V
+    stage_total_s = float(st.sum())
+    achieved = alg_bytes / stage_total_s / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                "kernel": "k_flow_stage_pair (3 RK3 stages per step)",
+                "bytes_per_site_step": sum(STAGE_BYTES_FP32), "peak_source": peak_kind,
+                "stage_ms": [round(x * 1e3, 4) for x in st]}
+
+    # FP64 flow for comparison (same field)
+    L64 = g.Lattice(DIMS, beta=BETA, precision="fp64", flow_eps=FLOW_EPS, seed=1, stream_id=rank, device=local)
+    L64.set_links(start)
+    s64 = torch.cuda.ExternalStream(L64.stream)
+    L64.flow(2, measure=True)
+    k64 = max(3, args.steps // 4)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s64)
+    L64.flow(k64, measure=True)
+    e1.record(s64)
+    torch.cuda.synchronize()
+    t64 = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+    rate64 = world * V * k64 / t64
+    L64.close()
+
+    # end to end through the C ABI: pinned host field in, host observables out
+    host_in = torch.from_numpy(start.reshape(-1)).pin_memory()
+    obs_e2e = torch.empty(((args.steps + 1) * (3 + DIMS[3]),), dtype=torch.float64).pin_memory()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L.flow_configuration_ptr(host_in.data_ptr(), args.steps, obs_e2e.data_ptr())
+    t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = {"value": world * V * args.steps / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": int(host_in.numel() * 8 / args.steps),
+           "d2h_bytes_per_step": int(obs_e2e.numel() * 8 / args.steps),
+           "how": "glac_flow_configuration: H2D of the FP64 host field, K steps with per-step observables, D2H"}
+    obs_last = obs_e2e.numpy().reshape(args.steps + 1, -1)[-1]
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_main / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Haar + 600 Metropolis sweeps)",
+        "config": {"workload": WORKLOAD, "dims": list(DIMS), "beta": BETA, "flow_eps": FLOW_EPS,
+                   "l2": "field 604 MB FP32 > 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"},
+        "roofline": roofline,
+        "cpu_baseline": cpu_base,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "extra": {
+            "flow_site_steps_per_s_no_obs": rate_noobs,
+            "flow_site_steps_per_s_fp64_with_obs": rate64,
+            "metropolis_link_updates_per_s_fp32": metro_rate,
+            "metropolis_acceptance": acc_holder.get("a"),
+            "plaq_after_flow": float(obs_last[0]),
+        },
+    }
+    if cpu_base:
+        line["extra"]["speedup_vs_cpu_baseline"] = value / cpu_base["value"]
+    if rank == 0:
+        print(json.dumps(line))
+    L.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    workers = os.cpu_count() or 1
+    kind = cpu_kind()
+    dims = (8, 8, 8, 16)
+    V = int(np.prod(dims))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers) as pool:
+        if args.warmup > 0:
+            pool.map(_cpu_worker, [(kind, dims, 1, 50 + i) for i in range(workers)])
+        t0 = time.perf_counter()
+        res = pool.map(_cpu_worker, [(kind, dims, args.steps, 1000 + i) for i in range(workers)])
+        wall = time.perf_counter() - t0
+    slowest = max(r[0] for r in res)
+    value = workers * V * args.steps / slowest
+    sample = (f"per step: each of {workers} processes runs 1 RK3 flow step + MasterSamplerTopcXYZ on its own "
+              f"{dims[0]}^3x{dims[3]} lattice ({'GLAC sources compiled as oracle/_ref' if kind == 'reference' else 'oracle C port'})")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": slowest / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Haar)",
+            "config": {"workload": WORKLOAD, "dims": list(DIMS), "beta": BETA, "flow_eps": FLOW_EPS},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": round(wall, 2)}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=25)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,570 @@
+// C ABI (include/glac_b200.h): contexts, device buffers, stream, and the
+// sequencing of the hot-path kernels.
+#include "../../include/glac_b200.h"
+#include "kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+using namespace glac;
+
+struct glac_ctx {
+    glac_desc d;
+    Geom g;
+    ObsPlan plan;
+    cudaStream_t stream = nullptr;
+    void *field[2] = {nullptr, nullptr};
+    int cur = 0;
+    void *force = nullptr;
+    double *partial = nullptr;
+    double *obs_dev = nullptr;
+    size_t obs_cap = 0;  // doubles in obs_dev
+    unsigned long long *acc_dev = nullptr;
+    double *staging = nullptr;
+    double *scalar_dev = nullptr;
+    uint32_t sweep = 0;
+    uint64_t launches = 0;
+    bool has_field = false;
+    bool pair_kernel = true;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_global_err;
+
+struct CudaError : std::exception {
+    std::string msg;
+    explicit CudaError(std::string m) : msg(std::move(m)) {}
+    const char *what() const noexcept override { return msg.c_str(); }
+};
+
+void ck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+void ck_launch(const char *what) { ck(cudaGetLastError(), what); }
+
+size_t field_bytes(const glac_desc &d, const Geom &g) {
+    return (size_t)g.V * 4 * 18 * (d.precision == GLAC_FP64 ? sizeof(double) : sizeof(float));
+}
+size_t force_bytes(const glac_desc &d, const Geom &g) {
+    return (size_t)g.V * 4 * 8 * (d.precision == GLAC_FP64 ? sizeof(double) : sizeof(float));
+}
+
+LinkField<double> f64(glac_ctx *c, int i) {
+    LinkField<double> L;
+    L.p = reinterpret_cast<double2 *>(c->field[i]);
+    L.Vh = c->g.Vh;
+    return L;
+}
+LinkField<float> f32(glac_ctx *c, int i) {
+    LinkField<float> L;
+    L.p4 = reinterpret_cast<float4 *>(c->field[i]);
+    L.p2 = reinterpret_cast<float2 *>(L.p4 + (size_t)16 * c->g.V);
+    L.Vh = c->g.Vh;
+    return L;
+}
+ForceField<double> z64(glac_ctx *c) {
+    ForceField<double> Z;
+    Z.p = reinterpret_cast<double2 *>(c->force);
+    Z.Vh = c->g.Vh;
+    return Z;
+}
+ForceField<float> z32(glac_ctx *c) {
+    ForceField<float> Z;
+    Z.p = reinterpret_cast<float4 *>(c->force);
+    Z.Vh = c->g.Vh;
+    return Z;
+}
+
+// Runs f with the context's device current; maps exceptions to a status.
+template <typename F>
+glac_status guarded(glac_ctx *c, F &&f) {
+    if (!c) return GLAC_ERR_ARG;
+    try {
+        ck(cudaSetDevice(c->d.device), "cudaSetDevice");
+        return f();
+    } catch (const CudaError &e) {
+        c->err = e.msg;
+        return GLAC_ERR_CUDA;
+    } catch (const std::exception &e) {
+        c->err = e.what();
+        return GLAC_ERR_ARG;
+    }
+}
+
+void ensure_staging(glac_ctx *c) {
+    if (!c->staging) ck(cudaMalloc(&c->staging, (size_t)c->g.V * 4 * 18 * sizeof(double)), "cudaMalloc staging");
+}
+void ensure_obs(glac_ctx *c, size_t n) {
+    if (c->obs_cap >= n) return;
+    if (c->obs_dev) cudaFree(c->obs_dev);
+    c->obs_dev = nullptr;
+    ck(cudaMalloc(&c->obs_dev, n * sizeof(double)), "cudaMalloc observables");
+    c->obs_cap = n;
+}
+
+void measure_into(glac_ctx *c, double *dev_out) {
+    if (c->d.precision == GLAC_FP64) launch_observables(c->g, f64(c, c->cur), c->plan, c->partial, dev_out, c->stream);
+    else launch_observables(c->g, f32(c, c->cur), c->plan, c->partial, dev_out, c->stream);
+    ck_launch("observables");
+    c->launches += 2;
+}
+
+void reunit(glac_ctx *c) {
+    if (c->d.precision == GLAC_FP64) launch_reunitarize(c->g, f64(c, c->cur), c->stream);
+    else launch_reunitarize(c->g, f32(c, c->cur), c->stream);
+    ck_launch("reunitarize");
+    c->launches += 1;
+}
+
+// One Luscher RK3 step: three fused stages, cur -> other -> cur -> other.
+// ev (optional) receives 4 events around the three stage launches.
+void flow_step(glac_ctx *c, cudaEvent_t *ev = nullptr) {
+    const double eps = c->d.flow_eps;
+    const double alpha[3] = {eps * 0.25, eps * 0.8888888888888888, 0.75 * eps};
+    const double beta[3] = {0.0, -(eps * 0.4722222222222222), -1.0};
+    if (ev) ck(cudaEventRecord(ev[0], c->stream), "event");
+    for (int stage = 0; stage < 3; stage++) {
+        const int src = c->cur, dst = c->cur ^ 1;
+        if (c->d.precision == GLAC_FP64) {
+            launch_flow_stage(c->g, f64(c, src), f64(c, dst), z64(c), stage, c->d.exp_func, alpha[stage],
+                              beta[stage], 128, c->stream);
+        } else if (c->pair_kernel && c->d.exp_func == GLAC_EXP_MORNINGSTAR) {
+            launch_flow_stage_pair(c->g, f32(c, src), f32(c, dst), z32(c), stage, alpha[stage], beta[stage], 128,
+                                   c->stream);
+        } else {
+            launch_flow_stage(c->g, f32(c, src), f32(c, dst), z32(c), stage, c->d.exp_func, alpha[stage],
+                              beta[stage], 128, c->stream);
+        }
+        ck_launch("flow stage");
+        c->launches += 1;
+        c->cur = dst;
+        if (ev) ck(cudaEventRecord(ev[stage + 1], c->stream), "event");
+    }
+}
+
+glac_status need_field(glac_ctx *c) {
+    if (!c->has_field) {
+        c->err = "no gauge field set (call glac_cold_start, glac_hot_start or glac_set_links first)";
+        return GLAC_ERR_STATE;
+    }
+    return GLAC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *glac_last_error(const glac_ctx *ctx) { return ctx ? ctx->err.c_str() : g_global_err.c_str(); }
+const char *glac_global_error(void) { return g_global_err.c_str(); }
+void *glac_stream(glac_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+uint64_t glac_launch_count(const glac_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+glac_status glac_create(const glac_desc *desc, glac_ctx **out) {
+    if (!desc || !out) { g_global_err = "null argument"; return GLAC_ERR_ARG; }
+    *out = nullptr;
+    const glac_desc &d = *desc;
+    long long V = 1;
+    for (int k = 0; k < 4; k++) {
+        if (d.dims[k] < 4 || (d.dims[k] & 1)) {
+            g_global_err = "every lattice extent must be even and at least 4";
+            return GLAC_ERR_ARG;
+        }
+        V *= d.dims[k];
+    }
+    if (V > (1ll << 29)) { g_global_err = "lattice too large (V > 2^29)"; return GLAC_ERR_ARG; }
+    if (d.precision != GLAC_FP64 && d.precision != GLAC_FP32) { g_global_err = "bad precision"; return GLAC_ERR_ARG; }
+    if (d.exp_func < 0 || d.exp_func > 3) { g_global_err = "bad exp_func"; return GLAC_ERR_ARG; }
+    if (d.n_updates < 0) { g_global_err = "n_updates must be >= 0"; return GLAC_ERR_ARG; }
+    if (!(d.su3_eps > 0.0 && d.su3_eps < 1.0)) { g_global_err = "su3_eps must lie in (0, 1)"; return GLAC_ERR_ARG; }
+    if (d.dims[3] > 1024) { g_global_err = "Nt > 1024 is not supported"; return GLAC_ERR_ARG; }
+    glac_ctx *c = new glac_ctx();
+    c->d = d;
+    c->g = make_geom(d.dims);
+    c->plan = make_obs_plan(c->g);
+    try {
+        ck(cudaSetDevice(d.device), "cudaSetDevice");
+        ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (int i = 0; i < 2; i++) ck(cudaMalloc(&c->field[i], field_bytes(d, c->g)), "cudaMalloc field");
+        ck(cudaMalloc(&c->force, force_bytes(d, c->g)), "cudaMalloc force");
+        ck(cudaMalloc(&c->partial, (size_t)3 * c->plan.nblocks * sizeof(double)), "cudaMalloc partials");
+        ck(cudaMalloc(&c->acc_dev, sizeof(unsigned long long)), "cudaMalloc counter");
+        ck(cudaMalloc(&c->scalar_dev, sizeof(double)), "cudaMalloc scalar");
+        ensure_obs(c, 3 + (size_t)d.dims[3]);
+    } catch (const CudaError &e) {
+        g_global_err = e.msg;
+        glac_destroy(c);
+        return GLAC_ERR_CUDA;
+    }
+    *out = c;
+    return GLAC_OK;
+}
+
+void glac_destroy(glac_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->d.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (int i = 0; i < 2; i++) if (c->field[i]) cudaFree(c->field[i]);
+    if (c->force) cudaFree(c->force);
+    if (c->partial) cudaFree(c->partial);
+    if (c->obs_dev) cudaFree(c->obs_dev);
+    if (c->acc_dev) cudaFree(c->acc_dev);
+    if (c->staging) cudaFree(c->staging);
+    if (c->scalar_dev) cudaFree(c->scalar_dev);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+glac_status glac_sync(glac_ctx *c) {
+    return guarded(c, [&] {
+        ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_set_option(glac_ctx *c, const char *key, long value) {
+    if (!c || !key) return GLAC_ERR_ARG;
+    if (!strcmp(key, "pair_kernel")) { c->pair_kernel = value != 0; return GLAC_OK; }
+    c->err = std::string("unknown option ") + key;
+    return GLAC_ERR_ARG;
+}
+
+glac_status glac_cold_start(glac_ctx *c) {
+    return guarded(c, [&] {
+        if (c->d.precision == GLAC_FP64) launch_cold(c->g, f64(c, c->cur), c->stream);
+        else launch_cold(c->g, f32(c, c->cur), c->stream);
+        ck_launch("cold start");
+        c->launches++;
+        c->has_field = true;
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_hot_start(glac_ctx *c, uint64_t seed) {
+    return guarded(c, [&] {
+        if (c->d.precision == GLAC_FP64) launch_haar(c->g, f64(c, c->cur), seed, c->d.stream_id, c->stream);
+        else launch_haar(c->g, f32(c, c->cur), seed, c->d.stream_id, c->stream);
+        ck_launch("hot start");
+        c->launches++;
+        c->has_field = true;
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_set_links_device(glac_ctx *c, const double *dev) {
+    return guarded(c, [&] {
+        if (!dev) { c->err = "null field"; return GLAC_ERR_ARG; }
+        if (c->d.precision == GLAC_FP64) launch_aos_to_soa(c->g, dev, f64(c, c->cur), c->stream);
+        else launch_aos_to_soa(c->g, dev, f32(c, c->cur), c->stream);
+        ck_launch("aos->soa");
+        c->launches++;
+        c->has_field = true;
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_get_links_device(glac_ctx *c, double *dev) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        if (c->d.precision == GLAC_FP64) launch_soa_to_aos(c->g, f64(c, c->cur), dev, c->stream);
+        else launch_soa_to_aos(c->g, f32(c, c->cur), dev, c->stream);
+        ck_launch("soa->aos");
+        c->launches++;
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_set_links(glac_ctx *c, const double *host) {
+    return guarded(c, [&] {
+        if (!host) { c->err = "null field"; return GLAC_ERR_ARG; }
+        ensure_staging(c);
+        ck(cudaMemcpyAsync(c->staging, host, (size_t)c->g.V * 72 * sizeof(double), cudaMemcpyHostToDevice,
+                           c->stream),
+           "H2D links");
+        glac_status s = glac_set_links_device(c, c->staging);
+        if (s != GLAC_OK) return s;
+        ck(cudaStreamSynchronize(c->stream), "sync");
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_get_links(glac_ctx *c, double *host) {
+    return guarded(c, [&] {
+        if (!host) { c->err = "null field"; return GLAC_ERR_ARG; }
+        ensure_staging(c);
+        glac_status s = glac_get_links_device(c, c->staging);
+        if (s != GLAC_OK) return s;
+        ck(cudaMemcpyAsync(host, c->staging, (size_t)c->g.V * 72 * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream),
+           "D2H links");
+        ck(cudaStreamSynchronize(c->stream), "sync");
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_reunitarize(glac_ctx *c) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        reunit(c);
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_unitarity_violation(glac_ctx *c, double *out) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        if (c->d.precision == GLAC_FP64) launch_max_unitarity_dev(c->g, f64(c, c->cur), c->scalar_dev, c->stream);
+        else launch_max_unitarity_dev(c->g, f32(c, c->cur), c->scalar_dev, c->stream);
+        ck_launch("unitarity");
+        c->launches++;
+        ck(cudaMemcpyAsync(out, c->scalar_dev, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "sync");
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_metropolis(glac_ctx *c, int n_sweeps, double *acceptance) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        if (n_sweeps < 0) { c->err = "n_sweeps < 0"; return GLAC_ERR_ARG; }
+        ck(cudaMemsetAsync(c->acc_dev, 0, sizeof(unsigned long long), c->stream), "memset");
+        for (int i = 0; i < n_sweeps; i++) {
+            for (int k = 0; k < 8; k++) {
+                const int mu = k >> 1, p = k & 1;
+                if (c->d.precision == GLAC_FP64)
+                    launch_metropolis(c->g, f64(c, c->cur), mu, p, c->d.beta, c->d.su3_eps, c->d.n_updates,
+                                      c->d.seed, c->sweep, c->d.stream_id, c->acc_dev, 128, c->stream);
+                else
+                    launch_metropolis(c->g, f32(c, c->cur), mu, p, c->d.beta, c->d.su3_eps, c->d.n_updates,
+                                      c->d.seed, c->sweep, c->d.stream_id, c->acc_dev, 128, c->stream);
+                ck_launch("metropolis");
+                c->launches++;
+            }
+            c->sweep++;
+            if (c->d.reunit_interval > 0 && c->d.precision == GLAC_FP32 && c->sweep % c->d.reunit_interval == 0)
+                reunit(c);
+        }
+        if (acceptance) {
+            unsigned long long acc = 0;
+            ck(cudaMemcpyAsync(&acc, c->acc_dev, sizeof(acc), cudaMemcpyDeviceToHost, c->stream), "D2H");
+            ck(cudaStreamSynchronize(c->stream), "sync");
+            const double per = 4.0 * (double)c->d.n_updates * (double)c->g.V * (double)(n_sweeps > 0 ? n_sweeps : 1);
+            *acceptance = per > 0 ? (double)acc / per : 0.0;
+        }
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_measure(glac_ctx *c, double *obs) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        const size_t n = 3 + (size_t)c->g.N[3];
+        ensure_obs(c, n);
+        measure_into(c, c->obs_dev);
+        if (obs) {
+            ck(cudaMemcpyAsync(obs, c->obs_dev, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H obs");
+            ck(cudaStreamSynchronize(c->stream), "sync");
+        }
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_flow(glac_ctx *c, int n_steps, double *obs) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        if (n_steps < 0) { c->err = "n_steps < 0"; return GLAC_ERR_ARG; }
+        const size_t per = 3 + (size_t)c->g.N[3];
+        if (obs) {
+            ensure_obs(c, per * (size_t)(n_steps + 1));
+            measure_into(c, c->obs_dev);
+        }
+        for (int i = 0; i < n_steps; i++) {
+            flow_step(c);
+            if (c->d.reunit_interval > 0 && c->d.precision == GLAC_FP32 && (i + 1) % c->d.reunit_interval == 0)
+                reunit(c);
+            if (obs) measure_into(c, c->obs_dev + per * (size_t)(i + 1));
+        }
+        if (obs) {
+            ck(cudaMemcpyAsync(obs, c->obs_dev, per * (size_t)(n_steps + 1) * sizeof(double), cudaMemcpyDeviceToHost,
+                               c->stream),
+               "D2H obs");
+            ck(cudaStreamSynchronize(c->stream), "sync");
+        }
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_flow_stage_times(glac_ctx *c, int n_steps, double *seconds3) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        if (n_steps <= 0 || !seconds3) { c->err = "n_steps must be > 0"; return GLAC_ERR_ARG; }
+        cudaEvent_t ev[4];
+        for (int i = 0; i < 4; i++) ck(cudaEventCreate(&ev[i]), "event create");
+        double acc[3] = {0, 0, 0};
+        for (int k = 0; k < n_steps; k++) {
+            flow_step(c, ev);
+            ck(cudaEventSynchronize(ev[3]), "event sync");
+            for (int i = 0; i < 3; i++) {
+                float ms = 0.f;
+                ck(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "elapsed");
+                acc[i] += ms * 1e-3;
+            }
+        }
+        for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
+        for (int i = 0; i < 3; i++) seconds3[i] = acc[i] / n_steps;
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_flow_configuration(glac_ctx *c, const double *host_links, int n_steps, double *obs) {
+    glac_status s = glac_set_links(c, host_links);
+    if (s != GLAC_OK) return s;
+    return glac_flow(c, n_steps, obs);
+}
+
+glac_status glac_staples(glac_ctx *c, double *host_out) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        ensure_staging(c);
+        if (c->d.precision == GLAC_FP64) launch_staples_aos(c->g, f64(c, c->cur), c->staging, c->stream);
+        else launch_staples_aos(c->g, f32(c, c->cur), c->staging, c->stream);
+        ck_launch("staples");
+        c->launches++;
+        ck(cudaMemcpyAsync(host_out, c->staging, (size_t)c->g.V * 72 * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream),
+           "D2H");
+        ck(cudaStreamSynchronize(c->stream), "sync");
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_force(glac_ctx *c, double *host_out) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        ensure_staging(c);
+        if (c->d.precision == GLAC_FP64) launch_force_aos(c->g, f64(c, c->cur), c->staging, c->stream);
+        else launch_force_aos(c->g, f32(c, c->cur), c->staging, c->stream);
+        ck_launch("force");
+        c->launches++;
+        ck(cudaMemcpyAsync(host_out, c->staging, (size_t)c->g.V * 72 * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream),
+           "D2H");
+        ck(cudaStreamSynchronize(c->stream), "sync");
+        return GLAC_OK;
+    });
+}
+
+}  // extern "C"
+
+// Standalone batch entry points (no context): device buffers live for the call.
+namespace {
+template <typename F>
+glac_status standalone(F &&f) {
+    try {
+        return f();
+    } catch (const CudaError &e) {
+        g_global_err = e.msg;
+        return GLAC_ERR_CUDA;
+    } catch (const std::exception &e) {
+        g_global_err = e.what();
+        return GLAC_ERR_ARG;
+    }
+}
+struct DevBuf {
+    void *p = nullptr;
+    explicit DevBuf(size_t n) { ck(cudaMalloc(&p, n ? n : 1), "cudaMalloc"); }
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+}  // namespace
+
+extern "C" {
+
+glac_status glac_exp_batch(int precision, int exp_func, const double *host_in, long n, double *host_out) {
+    return standalone([&] {
+        if (n < 0 || (precision != GLAC_FP64 && precision != GLAC_FP32) || exp_func < 0 || exp_func > 3) {
+            g_global_err = "bad argument";
+            return GLAC_ERR_ARG;
+        }
+        if (n == 0) return GLAC_OK;
+        const size_t bytes = (size_t)n * 18 * sizeof(double);
+        DevBuf in(bytes), out(bytes);
+        ck(cudaMemcpy(in.p, host_in, bytes, cudaMemcpyHostToDevice), "H2D");
+        if (precision == GLAC_FP64) launch_exp_batch<double>(exp_func, (const double *)in.p, (double *)out.p, n, 0);
+        else launch_exp_batch<float>(exp_func, (const double *)in.p, (double *)out.p, n, 0);
+        ck_launch("exp batch");
+        ck(cudaMemcpy(host_out, out.p, bytes, cudaMemcpyDeviceToHost), "D2H");
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_delta_s_batch(int precision, double beta, long n, const double *host_U, const double *host_Uprime,
+                               const double *host_A, double *host_out) {
+    return standalone([&] {
+        if (n < 0 || (precision != GLAC_FP64 && precision != GLAC_FP32)) {
+            g_global_err = "bad argument";
+            return GLAC_ERR_ARG;
+        }
+        if (n == 0) return GLAC_OK;
+        const size_t mb = (size_t)n * 18 * sizeof(double);
+        DevBuf U(mb), Up(mb), A(mb), out((size_t)n * sizeof(double));
+        ck(cudaMemcpy(U.p, host_U, mb, cudaMemcpyHostToDevice), "H2D");
+        ck(cudaMemcpy(Up.p, host_Uprime, mb, cudaMemcpyHostToDevice), "H2D");
+        ck(cudaMemcpy(A.p, host_A, mb, cudaMemcpyHostToDevice), "H2D");
+        if (precision == GLAC_FP64)
+            launch_delta_s<double>(beta, n, (const double *)U.p, (const double *)Up.p, (const double *)A.p,
+                                   (double *)out.p, 0);
+        else
+            launch_delta_s<float>(beta, n, (const double *)U.p, (const double *)Up.p, (const double *)A.p,
+                                  (double *)out.p, 0);
+        ck_launch("delta S");
+        ck(cudaMemcpy(host_out, out.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_accept_fed(int precision, double beta, long n_links, int n_hits, double *host_U,
+                            const double *host_A, const double *host_X, const double *host_r,
+                            unsigned char *host_accept) {
+    return standalone([&] {
+        if (n_links < 0 || n_hits < 0 || (precision != GLAC_FP64 && precision != GLAC_FP32)) {
+            g_global_err = "bad argument";
+            return GLAC_ERR_ARG;
+        }
+        if (n_links == 0) return GLAC_OK;
+        const size_t mb = (size_t)n_links * 18 * sizeof(double);
+        const size_t xb = mb * (size_t)n_hits, rb = (size_t)n_links * n_hits * sizeof(double);
+        const size_t ab = (size_t)n_links * n_hits;
+        DevBuf U(mb), A(mb), X(xb), r(rb), acc(ab);
+        ck(cudaMemcpy(U.p, host_U, mb, cudaMemcpyHostToDevice), "H2D");
+        ck(cudaMemcpy(A.p, host_A, mb, cudaMemcpyHostToDevice), "H2D");
+        if (xb) ck(cudaMemcpy(X.p, host_X, xb, cudaMemcpyHostToDevice), "H2D");
+        if (rb) ck(cudaMemcpy(r.p, host_r, rb, cudaMemcpyHostToDevice), "H2D");
+        if (precision == GLAC_FP64)
+            launch_accept_fed<double>(beta, n_links, n_hits, (double *)U.p, (const double *)A.p, (const double *)X.p,
+                                      (const double *)r.p, (unsigned char *)acc.p, 0);
+        else
+            launch_accept_fed<float>(beta, n_links, n_hits, (double *)U.p, (const double *)A.p, (const double *)X.p,
+                                     (const double *)r.p, (unsigned char *)acc.p, 0);
+        ck_launch("accept fed");
+        ck(cudaMemcpy(host_U, U.p, mb, cudaMemcpyDeviceToHost), "D2H");
+        if (ab) ck(cudaMemcpy(host_accept, acc.p, ab, cudaMemcpyDeviceToHost), "D2H");
+        return GLAC_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,768 @@
+// Hot-path kernels for sm_100a: fused flow stage, checkerboard Metropolis,
+// fused clover observables with deterministic FP64 reductions, plus field
+// initialisation, reunitarisation and layout conversion.
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <stdexcept>
+
+namespace glac {
+
+// ---------------------------------------------------------------------------
+// Flow stage (GLAC/flow/flow.cpp:43-73 with getActionDerivative,
+// GLAC/actions/wilsongaugeaction.cpp:55-86), one fused pass per RK3 stage:
+//   Z = P_ah(U_mu(n) A_mu(n)),  M = alpha Z + beta Zprev,  U' = exp(M) U.
+//   stage 0: M = (eps/4) Z0, stores Z0
+//   stage 1: M = (8/9 eps) Z1 - (17/36 eps) Z0, stores M
+//   stage 2: M = (3/4 eps) Z2 - M_prev
+// Reads field `in`, writes `out` (all four Z_mu come from the same field).
+// grid: x over the Vh sites of a parity plane, y = mu*2 + parity.
+// ---------------------------------------------------------------------------
+template <typename T, int KIND, int STAGE>
+__global__ void __launch_bounds__(128) k_flow_stage(Geom g, LinkField<T> in, LinkField<T> out, ForceField<T> zf,
+                                                    T alpha, T beta) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    const Site n = site_from_ps(g, p, s);
+    M3<T> A = staple(in, g, n, p, mu);
+    const M3<T> U = in.load(mu, p, s);
+    const AH8<T> Z = project_ah(mul(U, A));
+    AH8<T> M;
+    if (STAGE == 0) {
+        M = ah_scale(alpha, Z);
+        zf.store(mu, p, s, Z);
+    } else {
+        const AH8<T> W = zf.load(mu, p, s);
+        M = ah_axpby(alpha, Z, beta, W);
+        if (STAGE == 1) zf.store(mu, p, s, M);
+    }
+    out.store(mu, p, s, mul(expm<T>(KIND, M), U));
+}
+
+template <typename T>
+void launch_flow_stage(const Geom &g, const LinkField<T> &in, const LinkField<T> &out, const ForceField<T> &zf,
+                       int stage, int kind, double alpha, double beta, int block, cudaStream_t st) {
+    (void)block;
+    dim3 grid((g.Vh + 127) / 128, 8);
+    T a = (T)alpha, b = (T)beta;
+#define GLAC_FLOW_CASE(K, S) \
+    if (kind == K && stage == S) { k_flow_stage<T, K, S><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); return; }
+    GLAC_FLOW_CASE(0, 0) GLAC_FLOW_CASE(0, 1) GLAC_FLOW_CASE(0, 2)
+    GLAC_FLOW_CASE(1, 0) GLAC_FLOW_CASE(1, 1) GLAC_FLOW_CASE(1, 2)
+    GLAC_FLOW_CASE(2, 0) GLAC_FLOW_CASE(2, 1) GLAC_FLOW_CASE(2, 2)
+    GLAC_FLOW_CASE(3, 0) GLAC_FLOW_CASE(3, 1) GLAC_FLOW_CASE(3, 2)
+#undef GLAC_FLOW_CASE
+    throw std::invalid_argument("bad flow stage or exp kind");
+}
+template void launch_flow_stage<double>(const Geom &, const LinkField<double> &, const LinkField<double> &,
+                                        const ForceField<double> &, int, int, double, double, int, cudaStream_t);
+template void launch_flow_stage<float>(const Geom &, const LinkField<float> &, const LinkField<float> &,
+                                       const ForceField<float> &, int, int, double, double, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Packed-FP32 flow stage: each thread carries two sites of the same (mu, parity)
+// plane in the two lanes of f32x2, so every FP32 FMA of the SU(3) algebra is
+// one fma.rn.f32x2.  Lane sites: s and s + blockDim.x within a 2*blockDim.x tile.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ M3<f32x2> pack2(const M3<float> &a, const M3<float> &b) {
+    M3<f32x2> r;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        r.e[k].re = f32x2(a.e[k].re, b.e[k].re);
+        r.e[k].im = f32x2(a.e[k].im, b.e[k].im);
+    }
+    return r;
+}
+__device__ __forceinline__ void unpack2(const M3<f32x2> &r, M3<float> &a, M3<float> &b) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        a.e[k].re = r.e[k].re.v.x; a.e[k].im = r.e[k].im.v.x;
+        b.e[k].re = r.e[k].re.v.y; b.e[k].im = r.e[k].im.v.y;
+    }
+}
+__device__ __forceinline__ AH8<f32x2> pack2(const AH8<float> &a, const AH8<float> &b) {
+    AH8<f32x2> r;
+    r.a = f32x2(a.a, b.a); r.d = f32x2(a.d, b.d);
+    r.b = cx(f32x2(a.b.re, b.b.re), f32x2(a.b.im, b.b.im));
+    r.c = cx(f32x2(a.c.re, b.c.re), f32x2(a.c.im, b.c.im));
+    r.e = cx(f32x2(a.e.re, b.e.re), f32x2(a.e.im, b.e.im));
+    return r;
+}
+__device__ __forceinline__ void unpack2(const AH8<f32x2> &r, AH8<float> &a, AH8<float> &b) {
+    a.a = r.a.v.x; b.a = r.a.v.y; a.d = r.d.v.x; b.d = r.d.v.y;
+    a.b = cx(r.b.re.v.x, r.b.im.v.x); b.b = cx(r.b.re.v.y, r.b.im.v.y);
+    a.c = cx(r.c.re.v.x, r.c.im.v.x); b.c = cx(r.c.re.v.y, r.c.im.v.y);
+    a.e = cx(r.e.re.v.x, r.e.im.v.x); b.e = cx(r.e.re.v.y, r.e.im.v.y);
+}
+
+__device__ __forceinline__ M3<f32x2> staple_pair(const LinkField<float> &L, const Geom &g, const Site &n0,
+                                                 const Site &n1, int p, int mu) {
+    M3<f32x2> A;
+    set_zero(A);
+    const int q = p ^ 1;
+    const int a_mu = lex_step(g, n0, mu, +1) >> 1, b_mu = lex_step(g, n1, mu, +1) >> 1;
+#pragma unroll 1
+    for (int nu = 0; nu < 4; nu++) {
+        if (nu == mu) continue;
+        const int a_nup = lex_step(g, n0, nu, +1) >> 1, b_nup = lex_step(g, n1, nu, +1) >> 1;
+        const int a_num = lex_step(g, n0, nu, -1) >> 1, b_num = lex_step(g, n1, nu, -1) >> 1;
+        const int a_dg = lex_step2(g, n0, mu, +1, nu, -1) >> 1, b_dg = lex_step2(g, n1, mu, +1, nu, -1) >> 1;
+        {
+            M3<f32x2> a = pack2(L.load(nu, q, a_mu), L.load(nu, q, b_mu));
+            M3<f32x2> b = pack2(L.load(mu, q, a_nup), L.load(mu, q, b_nup));
+            M3<f32x2> t = mul_nd(a, b);
+            M3<f32x2> c = pack2(L.load(nu, p, n0.lex >> 1), L.load(nu, p, n1.lex >> 1));
+            acc_mul_nd(A, t, c);
+        }
+        {
+            M3<f32x2> a = pack2(L.load(nu, p, a_dg), L.load(nu, p, b_dg));
+            M3<f32x2> b = pack2(L.load(mu, q, a_num), L.load(mu, q, b_num));
+            M3<f32x2> t = mul_dd(a, b);
+            M3<f32x2> c = pack2(L.load(nu, q, a_num), L.load(nu, q, b_num));
+            acc_mul(A, t, c);
+        }
+    }
+    return A;
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(128) k_flow_stage_pair(Geom g, LinkField<float> in, LinkField<float> out,
+                                                         ForceField<float> zf, float alpha, float beta) {
+    const int s0 = blockIdx.x * (2 * blockDim.x) + threadIdx.x;
+    if (s0 >= g.Vh) return;
+    const bool has1 = s0 + (int)blockDim.x < g.Vh;
+    const int s1 = has1 ? s0 + (int)blockDim.x : s0;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    const Site n0 = site_from_ps(g, p, s0), n1 = site_from_ps(g, p, s1);
+    M3<f32x2> A = staple_pair(in, g, n0, n1, p, mu);
+    const M3<f32x2> U = pack2(in.load(mu, p, s0), in.load(mu, p, s1));
+    const AH8<f32x2> Z = project_ah(mul(U, A));
+    AH8<f32x2> M;
+    if (STAGE == 0) {
+        M = ah_scale(f32x2(alpha), Z);
+        AH8<float> z0, z1;
+        unpack2(Z, z0, z1);
+        zf.store(mu, p, s0, z0);
+        if (has1) zf.store(mu, p, s1, z1);
+    } else {
+        const AH8<f32x2> W = pack2(zf.load(mu, p, s0), zf.load(mu, p, s1));
+        M = ah_axpby(f32x2(alpha), Z, f32x2(beta), W);
+        if (STAGE == 1) {
+            AH8<float> m0, m1;
+            unpack2(M, m0, m1);
+            zf.store(mu, p, s0, m0);
+            if (has1) zf.store(mu, p, s1, m1);
+        }
+    }
+    M3<float> u0, u1;
+    unpack2(mul(expm_morningstar_pair(M), U), u0, u1);
+    out.store(mu, p, s0, u0);
+    if (has1) out.store(mu, p, s1, u1);
+}
+
+void launch_flow_stage_pair(const Geom &g, const LinkField<float> &in, const LinkField<float> &out,
+                            const ForceField<float> &zf, int stage, double alpha, double beta, int block,
+                            cudaStream_t st) {
+    (void)block;
+    dim3 grid((g.Vh + 255) / 256, 8);
+    float a = (float)alpha, b = (float)beta;
+    if (stage == 0) k_flow_stage_pair<0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b);
+    else if (stage == 1) k_flow_stage_pair<1><<<grid, 128, 0, st>>>(g, in, out, zf, a, b);
+    else k_flow_stage_pair<2><<<grid, 128, 0, st>>>(g, in, out, zf, a, b);
+}
+
+// ---------------------------------------------------------------------------
+// Checkerboard Metropolis sub-sweep over the links (mu, parity p).
+// Staple once per link, then nhits proposals U' = X U with X = R S T or its
+// inverse (GLAC/math/matrices/su3matrixgenerator.h:170-321), accepted iff
+// exp(-dS) > r with dS = -(beta/3) ReTr[(U' - U) A] (GLAC/system.cpp:333-361,
+// GLAC/actions/wilsongaugeaction.cpp:24-27).  The links of one (mu, parity)
+// class do not enter each other's staples, so they update concurrently.
+// Random numbers: Philox4x32-10, key = seed, counter = {4 hit + call,
+// mu V + lex, sweep, stream}; words 0-11 build R, S, T, word 12 picks X or
+// X^+, words 13-14 give the 53-bit accept uniform.
+// ---------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ T su_scalar(double v);
+template <> __device__ __forceinline__ double su_scalar<double>(double v) { return v; }
+template <> __device__ __forceinline__ float su_scalar<float>(double v) { return (float)v; }
+
+template <typename T>
+__device__ __forceinline__ void su2_near_unity(T u0, T u1, T u2, T u3, T eps, T sq1me, T out[4]) {
+    // x0 = sign(u0) sqrt(1 - eps^2), x = eps u / |u|, normalised
+    // (GLAC/math/matrices/su3matrixgenerator.h:202-243)
+    T x0 = u0 < T(0) ? -sq1me : sq1me;
+    T rn = sqrt(u1 * u1 + u2 * u2 + u3 * u3) / eps;
+    T x1 = u1 / rn, x2 = u2 / rn, x3 = u3 / rn;
+    T nrm = sqrt(x0 * x0 + x1 * x1 + x2 * x2 + x3 * x3);
+    out[0] = x0 / nrm; out[1] = x1 / nrm; out[2] = x2 / nrm; out[3] = x3 / nrm;
+}
+
+// X = R S T with R, S, T the SU(2) elements [[x0 + i x3, x2 + i x1], [-x2 + i x1, x0 - i x3]]
+// embedded in the (12), (13), (23) blocks; inverse -> X^+.
+template <typename T>
+__device__ __forceinline__ M3<T> rst_matrix(const T r[4], const T s[4], const T t[4], bool inverse) {
+    M3<T> R, S, Tm;
+    set_zero(R); set_zero(S); set_zero(Tm);
+    R(0, 0) = cx(r[0], r[3]); R(0, 1) = cx(r[2], r[1]); R(1, 0) = cx(-r[2], r[1]); R(1, 1) = cx(r[0], -r[3]);
+    R(2, 2).re = T(1);
+    S(0, 0) = cx(s[0], s[3]); S(0, 2) = cx(s[2], s[1]); S(2, 0) = cx(-s[2], s[1]); S(2, 2) = cx(s[0], -s[3]);
+    S(1, 1).re = T(1);
+    Tm(1, 1) = cx(t[0], t[3]); Tm(1, 2) = cx(t[2], t[1]); Tm(2, 1) = cx(-t[2], t[1]); Tm(2, 2) = cx(t[0], -t[3]);
+    Tm(0, 0).re = T(1);
+    M3<T> X = mul(mul(R, S), Tm);
+    return inverse ? dagger(X) : X;
+}
+
+template <typename T>
+__device__ __forceinline__ void draw_proposal(uint32_t k0, uint32_t k1, uint32_t link_id, uint32_t sweep,
+                                              uint32_t stream_id, int hit, T eps, T sq1me, M3<T> &X, double &r) {
+    uint32_t w[16];
+#pragma unroll
+    for (int call = 0; call < 4; call++) {
+        U4 c = {(uint32_t)(4 * hit + call), link_id, sweep, stream_id};
+        U4 o = philox4x32_10(c, k0, k1);
+        w[4 * call] = o.x; w[4 * call + 1] = o.y; w[4 * call + 2] = o.z; w[4 * call + 3] = o.w;
+    }
+    T su[3][4];
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+        su2_near_unity<T>(su_scalar<T>(u_sym(w[4 * b])), su_scalar<T>(u_sym(w[4 * b + 1])),
+                          su_scalar<T>(u_sym(w[4 * b + 2])), su_scalar<T>(u_sym(w[4 * b + 3])), eps, sq1me, su[b]);
+    X = rst_matrix<T>(su[0], su[1], su[2], (w[12] & 0x80000000u) == 0u);
+    r = u_53(w[13], w[14]);
+}
+
+template <typename T> __device__ __forceinline__ double accept_weight(T dS);
+template <> __device__ __forceinline__ double accept_weight<double>(double dS) { return exp(-dS); }
+template <> __device__ __forceinline__ double accept_weight<float>(float dS) { return (double)expf(-dS); }
+
+template <typename T>
+__device__ __forceinline__ T delta_s(const M3<T> &U, const M3<T> &Up, const M3<T> &A, T mfac) {
+    M3<T> D = Up;
+    sub_from(D, U);
+    return retr_mul(D, A) * mfac;
+}
+
+__device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned long long *dst) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __shared__ unsigned long long warp_sum[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) warp_sum[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        v = lane < nw ? warp_sum[lane] : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(dst, v);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_metropolis(Geom g, LinkField<T> L, int mu, int p, T mfac, T eps, T sq1me,
+                                                    int nhits, uint32_t k0, uint32_t k1, uint32_t sweep,
+                                                    uint32_t stream_id, unsigned long long *acc) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long na = 0;
+    if (s < g.Vh) {
+        const Site n = site_from_ps(g, p, s);
+        const M3<T> A = staple(L, g, n, p, mu);
+        M3<T> U = L.load_rw(mu, p, s);
+        const uint32_t link_id = (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex;
+#pragma unroll 1
+        for (int h = 0; h < nhits; h++) {
+            M3<T> X;
+            double r;
+            draw_proposal<T>(k0, k1, link_id, sweep, stream_id, h, eps, sq1me, X, r);
+            const M3<T> Up = mul(X, U);
+            if (accept_weight<T>(delta_s(U, Up, A, mfac)) > r) {
+                U = Up;
+                na++;
+            }
+        }
+        L.store(mu, p, s, U);
+    }
+    block_add_u64(na, acc);
+}
+
+template <typename T>
+void launch_metropolis(const Geom &g, const LinkField<T> &L, int mu, int p, double beta, double eps, int nhits,
+                       uint64_t seed, uint32_t sweep, uint32_t stream_id, unsigned long long *acc, int block,
+                       cudaStream_t st) {
+    (void)block;
+    const int B = 128;
+    dim3 grid((g.Vh + B - 1) / B);
+    k_metropolis<T><<<grid, B, 0, st>>>(g, L, mu, p, (T)(-beta / 3.0), (T)eps, (T)sqrt(1.0 - eps * eps), nhits,
+                                        (uint32_t)seed, (uint32_t)(seed >> 32), sweep, stream_id, acc);
+}
+template void launch_metropolis<double>(const Geom &, const LinkField<double> &, int, int, double, double, int,
+                                        uint64_t, uint32_t, uint32_t, unsigned long long *, int, cudaStream_t);
+template void launch_metropolis<float>(const Geom &, const LinkField<float> &, int, int, double, double, int,
+                                       uint64_t, uint32_t, uint32_t, unsigned long long *, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Observables (GLAC/observables/mastersamplertopcxyz.cpp:236-384): per site,
+// for nu = 1..3 and its cyclic complement (rho, sigma), the clovers
+//   C = leaf1 - leaf2 + leaf3 - leaf4 projected to (C - C^+) - 1/3 i ImTr,
+// plaq += ReTr leaf1, q(t) -= ReTr(C_0nu C_rhosigma), E += ReTr(C C) for both.
+// Every block lies in one (t, parity) half-slice, so the block sums are
+// per-time-slice partials; FP64 throughout the reduction, fixed order.
+// ---------------------------------------------------------------------------
+ObsPlan make_obs_plan(const Geom &g) {
+    const int half_slice = g.N[0] * g.N[1] * g.N[2] / 2;
+    int best = -1, best_score = 1 << 30;
+    for (int B = 1; B <= 256 && B <= half_slice; B++) {
+        if (half_slice % B) continue;
+        int score = (B % 32 == 0 ? 0 : 100000) + std::abs(B - 128);
+        if (score < best_score) { best_score = score; best = B; }
+    }
+    ObsPlan pl;
+    pl.Bv = best;
+    pl.B = (best + 31) / 32 * 32;
+    pl.nb = half_slice / best;
+    pl.nblocks = g.N[3] * 2 * pl.nb;
+    return pl;
+}
+
+template <typename T>
+__device__ __forceinline__ void clover(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu, int nu,
+                                       M3<T> &C, T &plaq) {
+    const int q = p ^ 1;
+    const int s_n = n.lex >> 1;
+    const int s_mup = lex_step(g, n, mu, +1) >> 1;           // n+mu      (q)
+    const int s_nup = lex_step(g, n, nu, +1) >> 1;           // n+nu      (q)
+    const int s_num = lex_step(g, n, nu, -1) >> 1;           // n-nu      (q)
+    const int s_mum = lex_step(g, n, mu, -1) >> 1;           // n-mu      (q)
+    const int s_pm = lex_step2(g, n, mu, +1, nu, -1) >> 1;   // n+mu-nu   (p)
+    const int s_mm = lex_step2(g, n, mu, -1, nu, -1) >> 1;   // n-mu-nu   (p)
+    const int s_mp = lex_step2(g, n, mu, -1, nu, +1) >> 1;   // n-mu+nu   (p)
+    const M3<T> Umu = L.load(mu, p, s_n);
+    const M3<T> Unu = L.load(nu, p, s_n);
+    // leaf1 = U_mu(n) U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+
+    {
+        M3<T> P = mul(Umu, L.load(nu, q, s_mup));
+        M3<T> W = mul(Unu, L.load(mu, q, s_nup));
+        C = mul_nd(P, W);
+        plaq = retr(C);
+    }
+    const M3<T> Unu_m = L.load(nu, q, s_num);  // U_nu(n-nu)
+    // leaf2 = U_mu(n) U_nu(n+mu-nu)^+ U_mu(n-nu)^+ U_nu(n-nu)
+    {
+        M3<T> Y = mul(L.load(mu, q, s_num), L.load(nu, p, s_pm));
+        sub_from(C, mul(mul_nd(Umu, Y), Unu_m));
+    }
+    const M3<T> Umu_m = L.load(mu, q, s_mum);  // U_mu(n-mu)
+    // leaf3 = U_mu(n-mu)^+ U_nu(n-mu-nu)^+ U_mu(n-mu-nu) U_nu(n-nu)
+    {
+        M3<T> t = mul_dd(Umu_m, L.load(nu, p, s_mm));
+        t = mul(t, L.load(mu, p, s_mm));
+        add_to(C, mul(t, Unu_m));
+    }
+    // leaf4 = U_mu(n-mu)^+ U_nu(n-mu) U_mu(n-mu+nu) U_nu(n)^+
+    {
+        M3<T> t = mul_dn(Umu_m, L.load(nu, q, s_mum));
+        t = mul(t, L.load(mu, p, s_mp));
+        sub_from(C, mul_nd(t, Unu));
+    }
+    // (C - C^+) - 1/3 i ImTr(C - C^+)
+    M3<T> D = dagger(C);
+    sub_from(C, D);
+    T tr = (C(0, 0).im + C(1, 1).im + C(2, 2).im) / T(3);
+    C(0, 0).im = C(0, 0).im - tr;
+    C(1, 1).im = C(1, 1).im - tr;
+    C(2, 2).im = C(2, 2).im - tr;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_observables(Geom g, LinkField<T> L, int nb, int Bv, double *partial) {
+    const int b = blockIdx.x;
+    const int t = b / (2 * nb);
+    const int p = (b / nb) & 1;
+    const int j = b % nb;
+    const int half_slice = g.Vh / g.N[3];
+    const bool valid = (int)threadIdx.x < Bv;
+    const int s = t * half_slice + j * Bv + (valid ? (int)threadIdx.x : 0);
+    double plaq = 0.0, en = 0.0, qt = 0.0;
+    const Site n = site_from_ps(g, p, s);
+#pragma unroll 1
+    for (int nu = 1; nu < 4 && valid; nu++) {
+        const int rho = nu % 3 + 1, sigma = rho % 3 + 1;
+        M3<T> C1, C2;
+        T pl1, pl2;
+        clover(L, g, n, p, 0, nu, C1, pl1);
+        clover(L, g, n, p, rho, sigma, C2, pl2);
+        plaq += (double)pl1 + (double)pl2;
+        qt -= (double)retr_mul(C1, C2);
+        en += (double)retr_mul(C1, C1) + (double)retr_mul(C2, C2);
+    }
+    // deterministic block reduction
+    __shared__ double sh[3][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    plaq = warp_sum_d(plaq);
+    en = warp_sum_d(en);
+    qt = warp_sum_d(qt);
+    if (lane == 0) { sh[0][wid] = plaq; sh[1][wid] = en; sh[2][wid] = qt; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double a = 0.0, e = 0.0, q = 0.0;
+        for (int w = 0; w < nw; w++) { a += sh[0][w]; e += sh[1][w]; q += sh[2][w]; }
+        partial[3 * b] = a;
+        partial[3 * b + 1] = e;
+        partial[3 * b + 2] = q;
+    }
+}
+
+// out = [plaq, topc, energy, topct[Nt]] with the reference's normalisations
+// (mastersamplertopcxyz.cpp:13-16, :363-383).
+__global__ void k_obs_finalize(int Nt, int nb, int V, const double *partial, double *out) {
+    __shared__ double sp[1024], se[1024], sq[1024];
+    for (int t = threadIdx.x; t < Nt; t += blockDim.x) {
+        double a = 0.0, e = 0.0, q = 0.0;
+        for (int k = 0; k < 2 * nb; k++) {
+            const double *pp = partial + 3 * ((size_t)t * 2 * nb + k);
+            a += pp[0];
+            e += pp[1];
+            q += pp[2];
+        }
+        sp[t] = a; se[t] = e; sq[t] = q;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double qfac = 1.0 / (16 * 16 * M_PI * M_PI);
+        double a = 0.0, e = 0.0, q = 0.0;
+        for (int t = 0; t < Nt; t++) { a += sp[t]; e += se[t]; q += sq[t]; }
+        out[0] = a / (18.0 * (double)V);
+        out[1] = q * qfac;
+        out[2] = e / (double)V;
+        for (int t = 0; t < Nt; t++) out[3 + t] = sq[t] * qfac;
+    }
+}
+
+template <typename T>
+void launch_observables(const Geom &g, const LinkField<T> &L, const ObsPlan &plan, double *partial, double *out,
+                        cudaStream_t st) {
+    if (g.N[3] > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
+    k_observables<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial);
+    k_obs_finalize<<<1, 256, 0, st>>>(g.N[3], plan.nb, g.V, partial, out);
+}
+template void launch_observables<double>(const Geom &, const LinkField<double> &, const ObsPlan &, double *,
+                                         double *, cudaStream_t);
+template void launch_observables<float>(const Geom &, const LinkField<float> &, const ObsPlan &, double *,
+                                        double *, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Start fields, reunitarisation, layout conversion
+// ---------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ M3<T> to_t(const M3<double> &a) {
+    M3<T> r;
+#pragma unroll
+    for (int k = 0; k < 9; k++) { r.e[k].re = (T)a.e[k].re; r.e[k].im = (T)a.e[k].im; }
+    return r;
+}
+template <typename T> __device__ __forceinline__ M3<double> to_d(const M3<T> &a) {
+    M3<double> r;
+#pragma unroll
+    for (int k = 0; k < 9; k++) { r.e[k].re = (double)a.e[k].re; r.e[k].im = (double)a.e[k].im; }
+    return r;
+}
+
+// grid: x over Vh, y = mu*2 + parity
+template <typename T>
+__global__ void k_haar(Geom g, LinkField<T> L, uint32_t k0, uint32_t k1, uint32_t stream_id) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    const Site n = site_from_ps(g, p, s);
+    const uint32_t link_id = (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex;
+    uint32_t w[20];
+#pragma unroll
+    for (int call = 0; call < 5; call++) {
+        U4 c = {(uint32_t)call, link_id, 0xA11Au, stream_id};
+        U4 o = philox4x32_10(c, k0, k1);
+        w[4 * call] = o.x; w[4 * call + 1] = o.y; w[4 * call + 2] = o.z; w[4 * call + 3] = o.w;
+    }
+    M3<double> Z;
+#pragma unroll
+    for (int e = 0; e < 9; e++) {  // Box-Muller
+        double u1 = ((double)w[2 * e] + 1.0) * 2.3283064365386963e-10;
+        double u2 = (double)w[2 * e + 1] * 2.3283064365386963e-10;
+        double rad = sqrt(-2.0 * log(u1));
+        double sn, cs;
+        sincospi(2.0 * u2, &sn, &cs);
+        Z.e[e] = cx(rad * cs, rad * sn);
+    }
+    // Gram-Schmidt on columns (QR with positive real R diagonal -> Haar on U(3))
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+#pragma unroll
+        for (int pc = 0; pc < j; pc++) {
+            Cx<double> d = cx(0.0, 0.0);
+#pragma unroll
+            for (int i = 0; i < 3; i++) d = cmac_cj(d, Z(i, pc), Z(i, j));
+#pragma unroll
+            for (int i = 0; i < 3; i++) Z(i, j) = Z(i, j) - d * Z(i, pc);
+        }
+        double nrm = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++) nrm += Z(i, j).re * Z(i, j).re + Z(i, j).im * Z(i, j).im;
+        nrm = rsqrt(nrm);
+#pragma unroll
+        for (int i = 0; i < 3; i++) Z(i, j) = cx(Z(i, j).re * nrm, Z(i, j).im * nrm);
+    }
+    Cx<double> det = cx(0.0, 0.0);
+#pragma unroll
+    for (int pc = 0; pc < 3; pc++) {
+        const int a = (pc + 1) % 3, b = (pc + 2) % 3;
+        det = det + Z(0, pc) * (Z(1, a) * Z(2, b) - Z(1, b) * Z(2, a));
+    }
+    double sn, cs;
+    sincos(-atan2(det.im, det.re) / 3.0, &sn, &cs);
+    const Cx<double> f = cx(cs, sn);
+#pragma unroll
+    for (int e = 0; e < 9; e++) Z.e[e] = Z.e[e] * f;
+    L.store(mu, p, s, to_t<T>(Z));
+}
+
+template <typename T>
+__global__ void k_cold(Geom g, LinkField<T> L) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    M3<T> I;
+    set_identity(I);
+    L.store(blockIdx.y >> 1, blockIdx.y & 1, s, I);
+}
+
+// Row Gram-Schmidt in FP64, third row = conj(row0 x row1).
+__device__ __forceinline__ M3<double> reunit(M3<double> U) {
+    double na = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; j++) na += U(0, j).re * U(0, j).re + U(0, j).im * U(0, j).im;
+    na = rsqrt(na);
+#pragma unroll
+    for (int j = 0; j < 3; j++) U(0, j) = cx(U(0, j).re * na, U(0, j).im * na);
+    Cx<double> d = cx(0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < 3; j++) d = cmac_cj(d, U(0, j), U(1, j));
+#pragma unroll
+    for (int j = 0; j < 3; j++) U(1, j) = U(1, j) - d * U(0, j);
+    double nb = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; j++) nb += U(1, j).re * U(1, j).re + U(1, j).im * U(1, j).im;
+    nb = rsqrt(nb);
+#pragma unroll
+    for (int j = 0; j < 3; j++) U(1, j) = cx(U(1, j).re * nb, U(1, j).im * nb);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int a = (j + 1) % 3, b = (j + 2) % 3;
+        U(2, j) = conj(U(0, a) * U(1, b) - U(0, b) * U(1, a));
+    }
+    return U;
+}
+
+template <typename T>
+__global__ void k_reunitarize(Geom g, LinkField<T> L) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    L.store(mu, p, s, to_t<T>(reunit(to_d(L.load_rw(mu, p, s)))));
+}
+
+// AoS host layout [mu][lex][18] (FP64) <-> SoA. grid: x over V, y = mu.
+template <typename T>
+__global__ void k_aos_to_soa(Geom g, const double *aos, LinkField<T> L) {
+    const int lex = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lex >= g.V) return;
+    const int mu = blockIdx.y;
+    const double2 *src = reinterpret_cast<const double2 *>(aos + ((size_t)mu * g.V + lex) * 18);
+    M3<double> U;
+#pragma unroll
+    for (int k = 0; k < 9; k++) { double2 v = src[k]; U.e[k] = cx(v.x, v.y); }
+    const int p = parity_of_lex(g, lex);
+    L.store(mu, p, lex >> 1, to_t<T>(U));
+}
+template <typename T>
+__global__ void k_soa_to_aos(Geom g, LinkField<T> L, double *aos) {
+    const int lex = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lex >= g.V) return;
+    const int mu = blockIdx.y;
+    const int p = parity_of_lex(g, lex);
+    const M3<double> U = to_d(L.load_rw(mu, p, lex >> 1));
+    double2 *dst = reinterpret_cast<double2 *>(aos + ((size_t)mu * g.V + lex) * 18);
+#pragma unroll
+    for (int k = 0; k < 9; k++) dst[k] = make_double2(U.e[k].re, U.e[k].im);
+}
+template <typename T>
+__global__ void k_copy_field(Geom g, LinkField<T> src, LinkField<T> dst) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    dst.store(mu, p, s, src.load_rw(mu, p, s));
+}
+
+template <typename T>
+void launch_haar(const Geom &g, const LinkField<T> &L, uint64_t seed, uint32_t stream_id, cudaStream_t st) {
+    k_haar<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L, (uint32_t)seed, (uint32_t)(seed >> 32), stream_id);
+}
+template <typename T>
+void launch_cold(const Geom &g, const LinkField<T> &L, cudaStream_t st) {
+    k_cold<T><<<dim3((g.Vh + 255) / 256, 8), 256, 0, st>>>(g, L);
+}
+template <typename T>
+void launch_reunitarize(const Geom &g, const LinkField<T> &L, cudaStream_t st) {
+    k_reunitarize<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L);
+}
+template <typename T>
+void launch_aos_to_soa(const Geom &g, const double *aos, const LinkField<T> &L, cudaStream_t st) {
+    k_aos_to_soa<T><<<dim3((g.V + 127) / 128, 4), 128, 0, st>>>(g, aos, L);
+}
+template <typename T>
+void launch_soa_to_aos(const Geom &g, const LinkField<T> &L, double *aos, cudaStream_t st) {
+    k_soa_to_aos<T><<<dim3((g.V + 127) / 128, 4), 128, 0, st>>>(g, L, aos);
+}
+template <typename T>
+void launch_copy_field(const Geom &g, const LinkField<T> &src, const LinkField<T> &dst, cudaStream_t st) {
+    k_copy_field<T><<<dim3((g.Vh + 255) / 256, 8), 256, 0, st>>>(g, src, dst);
+}
+
+// ---------------------------------------------------------------------------
+// Test exports
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_staples_aos(Geom g, LinkField<T> L, double *out, int force) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    const Site n = site_from_ps(g, p, s);
+    M3<T> A = staple(L, g, n, p, mu);
+    if (force) A = ah_to_m3(project_ah(mul(L.load(mu, p, s), A)));
+    const M3<double> Ad = to_d(A);
+    double2 *dst = reinterpret_cast<double2 *>(out + ((size_t)mu * g.V + n.lex) * 18);
+#pragma unroll
+    for (int k = 0; k < 9; k++) dst[k] = make_double2(Ad.e[k].re, Ad.e[k].im);
+}
+template <typename T>
+void launch_staples_aos(const Geom &g, const LinkField<T> &L, double *out, cudaStream_t st) {
+    k_staples_aos<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L, out, 0);
+}
+template <typename T>
+void launch_force_aos(const Geom &g, const LinkField<T> &L, double *out, cudaStream_t st) {
+    k_staples_aos<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L, out, 1);
+}
+
+template <typename T>
+__device__ __forceinline__ M3<T> load_aos(const double *p) {
+    M3<T> U;
+#pragma unroll
+    for (int k = 0; k < 9; k++) U.e[k] = cx((T)p[2 * k], (T)p[2 * k + 1]);
+    return U;
+}
+template <typename T>
+__device__ __forceinline__ void store_aos(double *p, const M3<T> &U) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) { p[2 * k] = (double)U.e[k].re; p[2 * k + 1] = (double)U.e[k].im; }
+}
+
+// exp of n anti-Hermitian traceless matrices given as full 18-double matrices;
+// the 8 independent reals are taken as the flow kernels store them.
+template <typename T>
+__global__ void k_exp_batch(int kind, const double *in, double *out, long n) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const M3<T> M = load_aos<T>(in + 18 * i);
+    AH8<T> Z;
+    Z.a = M(0, 0).im; Z.d = M(1, 1).im;
+    Z.b = M(0, 1); Z.c = M(0, 2); Z.e = M(1, 2);
+    store_aos(out + 18 * i, expm<T>(kind, Z));
+}
+template <typename T>
+void launch_exp_batch(int kind, const double *in, double *out, long n, cudaStream_t st) {
+    k_exp_batch<T><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(kind, in, out, n);
+}
+
+template <typename T>
+__global__ void k_accept_fed(T mfac, long nlinks, int nhits, double *U, const double *A, const double *X,
+                             const double *r, unsigned char *accept) {
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nlinks) return;
+    M3<T> u = load_aos<T>(U + 18 * k);
+    const M3<T> a = load_aos<T>(A + 18 * k);
+    for (int h = 0; h < nhits; h++) {
+        const M3<T> Up = mul(load_aos<T>(X + 18 * (k * nhits + h)), u);
+        const bool acc = accept_weight<T>(delta_s(u, Up, a, mfac)) > r[k * nhits + h];
+        accept[k * nhits + h] = acc ? 1 : 0;
+        if (acc) u = Up;
+    }
+    store_aos(U + 18 * k, u);
+}
+template <typename T>
+void launch_accept_fed(double beta, long nlinks, int nhits, double *U, const double *A, const double *X,
+                       const double *r, unsigned char *accept, cudaStream_t st) {
+    k_accept_fed<T><<<(unsigned)((nlinks + 127) / 128), 128, 0, st>>>((T)(-beta / 3.0), nlinks, nhits, U, A, X, r,
+                                                                       accept);
+}
+
+template <typename T>
+__global__ void k_delta_s(T mfac, long n, const double *U, const double *Up, const double *A, double *out) {
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    out[k] = (double)delta_s(load_aos<T>(U + 18 * k), load_aos<T>(Up + 18 * k), load_aos<T>(A + 18 * k), mfac);
+}
+template <typename T>
+void launch_delta_s(double beta, long n, const double *U, const double *Up, const double *A, double *out,
+                    cudaStream_t st) {
+    k_delta_s<T><<<(unsigned)((n + 127) / 128), 128, 0, st>>>((T)(-beta / 3.0), n, U, Up, A, out);
+}
+
+// max over links of |U U^+ - 1| (entrywise), FP64 result in out[0] via atomicMax on the bit pattern.
+template <typename T>
+__global__ void k_unitarity(Geom g, LinkField<T> L, unsigned long long *out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    const M3<double> U = to_d(L.load_rw(mu, p, s));
+    const M3<double> P = mul_nd(U, U);
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            double re = P(i, j).re - (i == j ? 1.0 : 0.0);
+            m = fmax(m, fmax(fabs(re), fabs(P(i, j).im)));
+        }
+    atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+template <typename T>
+void launch_max_unitarity_dev(const Geom &g, const LinkField<T> &L, double *out, cudaStream_t st) {
+    cudaMemsetAsync(out, 0, sizeof(double), st);
+    k_unitarity<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L, reinterpret_cast<unsigned long long *>(out));
+}
+
+#define GLAC_INST(T)                                                                                             \
+    template void launch_haar<T>(const Geom &, const LinkField<T> &, uint64_t, uint32_t, cudaStream_t);          \
+    template void launch_cold<T>(const Geom &, const LinkField<T> &, cudaStream_t);                              \
+    template void launch_reunitarize<T>(const Geom &, const LinkField<T> &, cudaStream_t);                       \
+    template void launch_aos_to_soa<T>(const Geom &, const double *, const LinkField<T> &, cudaStream_t);        \
+    template void launch_soa_to_aos<T>(const Geom &, const LinkField<T> &, double *, cudaStream_t);              \
+    template void launch_copy_field<T>(const Geom &, const LinkField<T> &, const LinkField<T> &, cudaStream_t);  \
+    template void launch_staples_aos<T>(const Geom &, const LinkField<T> &, double *, cudaStream_t);             \
+    template void launch_force_aos<T>(const Geom &, const LinkField<T> &, double *, cudaStream_t);               \
+    template void launch_exp_batch<T>(int, const double *, double *, long, cudaStream_t);                        \
+    template void launch_accept_fed<T>(double, long, int, double *, const double *, const double *,              \
+                                       const double *, unsigned char *, cudaStream_t);                           \
+    template void launch_max_unitarity_dev<T>(const Geom &, const LinkField<T> &, double *, cudaStream_t);      \
+    template void launch_delta_s<T>(double, long, const double *, const double *, const double *, double *,     \
+                                    cudaStream_t);
+GLAC_INST(double)
+GLAC_INST(float)
+#undef GLAC_INST
+
+}  // namespace glac

@@ -1,0 +1,269 @@
+// Lattice geometry, the HBM layout of gauge fields, and the Philox streams.
+//
+// Layout (structure of arrays, even/odd split): a field of 4 link directions
+// over V = Nx Ny Nz Nt sites is stored per (mu, parity) plane of Vh = V/2
+// sites, each link split into 16-byte chunks so that a warp reading 32
+// consecutive sites of one chunk issues fully coalesced 128-bit loads:
+//   FP64: 9 double2 chunks   chunk k = complex element k (row-major)
+//         addr = ((mu*2 + p)*9 + k)*Vh + s
+//   FP32: 4 float4 chunks (complex elements 2k, 2k+1) + 1 float2 chunk (element 8)
+//         addr4 = ((mu*2 + p)*4 + k)*Vh + s ,  addr2 = (mu*2 + p)*Vh + s
+// The site index inside a parity plane is s = lex >> 1 with
+// lex = x + Nx(y + Ny(z + Nz t)), the reference's site order
+// (GLAC/parallelization/index.h:32-35); Nx must be even.
+// Traceless anti-Hermitian flow forces use 8 reals per link (a, d, b, c, e):
+//   FP64: 4 double2 chunks, FP32: 2 float4 chunks, same plane ordering.
+#pragma once
+
+#include <stdint.h>
+#include "su3.cuh"
+
+namespace glac {
+
+// Division by a runtime constant via a multiply-high (Granlund & Montgomery,
+// PLDI'94): q = (umulhi(m, n) + n) >> l for n < 2^31.
+struct FastDiv {
+    uint32_t d, m, l;
+    FastDiv() {}
+    explicit FastDiv(uint32_t d_) : d(d_) {
+        l = 0;
+        while ((1ull << l) < d) l++;
+        m = (uint32_t)((((1ull << l) - d) << 32) / d + 1);
+    }
+};
+GLAC_HD uint32_t fdiv(uint32_t n, const FastDiv &f) {
+#ifdef __CUDA_ARCH__
+    return (__umulhi(f.m, n) + n) >> f.l;
+#else
+    return (uint32_t)((((uint64_t)f.m * n >> 32) + n) >> f.l);
+#endif
+}
+
+struct Geom {
+    int N[4];
+    int Nxh;
+    int Vh;
+    int V;
+    int stride[4];  // lexicographic strides 1, Nx, Nx Ny, Nx Ny Nz
+    FastDiv div_xh, div_y, div_z;
+};
+
+inline Geom make_geom(const int N[4]) {
+    Geom g;
+    for (int d = 0; d < 4; d++) g.N[d] = N[d];
+    g.Nxh = N[0] / 2;
+    g.V = N[0] * N[1] * N[2] * N[3];
+    g.Vh = g.V / 2;
+    g.stride[0] = 1;
+    g.stride[1] = N[0];
+    g.stride[2] = N[0] * N[1];
+    g.stride[3] = N[0] * N[1] * N[2];
+    g.div_xh = FastDiv((uint32_t)g.Nxh);
+    g.div_y = FastDiv((uint32_t)N[1]);
+    g.div_z = FastDiv((uint32_t)N[2]);
+    return g;
+}
+
+// Site with coordinates c[] and its lexicographic index.
+struct Site {
+    int c[4];
+    int lex;
+};
+
+// (parity, index in parity plane) -> coordinates
+GLAC_HD Site site_from_ps(const Geom &g, int p, int s) {
+    Site st;
+    uint32_t q = fdiv((uint32_t)s, g.div_xh);
+    int xh = s - (int)q * g.Nxh;
+    uint32_t q2 = fdiv(q, g.div_y);
+    st.c[1] = (int)(q - q2 * g.N[1]);
+    uint32_t q3 = fdiv(q2, g.div_z);
+    st.c[2] = (int)(q2 - q3 * g.N[2]);
+    st.c[3] = (int)q3;
+    st.c[0] = 2 * xh + ((st.c[1] + st.c[2] + st.c[3] + p) & 1);
+    st.lex = st.c[0] + g.N[0] * (st.c[1] + g.N[1] * (st.c[2] + g.N[2] * st.c[3]));
+    return st;
+}
+
+// lexicographic index of n + a e_d (a = +1 or -1), periodic
+GLAC_HD int lex_step(const Geom &g, const Site &n, int d, int a) {
+    int cd = n.c[d];
+    int off;
+    if (a > 0) off = (cd == g.N[d] - 1) ? -(g.N[d] - 1) * g.stride[d] : g.stride[d];
+    else off = (cd == 0) ? (g.N[d] - 1) * g.stride[d] : -g.stride[d];
+    return n.lex + off;
+}
+// lexicographic index of n + a e_d + b e_e (d != e)
+GLAC_HD int lex_step2(const Geom &g, const Site &n, int d, int a, int e, int b) {
+    int cd = n.c[d], ce = n.c[e];
+    int off;
+    if (a > 0) off = (cd == g.N[d] - 1) ? -(g.N[d] - 1) * g.stride[d] : g.stride[d];
+    else off = (cd == 0) ? (g.N[d] - 1) * g.stride[d] : -g.stride[d];
+    if (b > 0) off += (ce == g.N[e] - 1) ? -(g.N[e] - 1) * g.stride[e] : g.stride[e];
+    else off += (ce == 0) ? (g.N[e] - 1) * g.stride[e] : -g.stride[e];
+    return n.lex + off;
+}
+
+GLAC_HD int parity_of_lex(const Geom &g, int lex) {
+    // parity = (x+y+z+t) & 1; only needed on the host side, slow path
+    int x = lex % g.N[0];
+    int r = lex / g.N[0];
+    int y = r % g.N[1];
+    r /= g.N[1];
+    int z = r % g.N[2];
+    int t = r / g.N[2];
+    return (x + y + z + t) & 1;
+}
+
+// ---------------------------------------------------------------------------
+// Field accessors
+// ---------------------------------------------------------------------------
+template <typename T> struct LinkField;
+
+template <> struct LinkField<double> {
+    double2 *p;
+    int Vh;
+    GLAC_HD size_t at(int mu, int par, int k, int s) const {
+        return ((size_t)((mu * 2 + par) * 9 + k)) * (size_t)Vh + (size_t)s;
+    }
+    __device__ __forceinline__ M3<double> load(int mu, int par, int s) const {
+        M3<double> U;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            double2 v = __ldg(p + at(mu, par, k, s));
+            U.e[k].re = v.x; U.e[k].im = v.y;
+        }
+        return U;
+    }
+    __device__ __forceinline__ M3<double> load_rw(int mu, int par, int s) const {
+        M3<double> U;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            double2 v = p[at(mu, par, k, s)];
+            U.e[k].re = v.x; U.e[k].im = v.y;
+        }
+        return U;
+    }
+    __device__ __forceinline__ void store(int mu, int par, int s, const M3<double> &U) const {
+#pragma unroll
+        for (int k = 0; k < 9; k++) p[at(mu, par, k, s)] = make_double2(U.e[k].re, U.e[k].im);
+    }
+};
+
+template <> struct LinkField<float> {
+    float4 *p4;
+    float2 *p2;
+    int Vh;
+    GLAC_HD size_t at4(int mu, int par, int k, int s) const {
+        return ((size_t)((mu * 2 + par) * 4 + k)) * (size_t)Vh + (size_t)s;
+    }
+    GLAC_HD size_t at2(int mu, int par, int s) const { return ((size_t)(mu * 2 + par)) * (size_t)Vh + (size_t)s; }
+    __device__ __forceinline__ M3<float> load(int mu, int par, int s) const {
+        M3<float> U;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            float4 v = __ldg(p4 + at4(mu, par, k, s));
+            U.e[2 * k].re = v.x; U.e[2 * k].im = v.y; U.e[2 * k + 1].re = v.z; U.e[2 * k + 1].im = v.w;
+        }
+        float2 w = __ldg(p2 + at2(mu, par, s));
+        U.e[8].re = w.x; U.e[8].im = w.y;
+        return U;
+    }
+    __device__ __forceinline__ M3<float> load_rw(int mu, int par, int s) const {
+        M3<float> U;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            float4 v = p4[at4(mu, par, k, s)];
+            U.e[2 * k].re = v.x; U.e[2 * k].im = v.y; U.e[2 * k + 1].re = v.z; U.e[2 * k + 1].im = v.w;
+        }
+        float2 w = p2[at2(mu, par, s)];
+        U.e[8].re = w.x; U.e[8].im = w.y;
+        return U;
+    }
+    __device__ __forceinline__ void store(int mu, int par, int s, const M3<float> &U) const {
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            p4[at4(mu, par, k, s)] = make_float4(U.e[2 * k].re, U.e[2 * k].im, U.e[2 * k + 1].re, U.e[2 * k + 1].im);
+        p2[at2(mu, par, s)] = make_float2(U.e[8].re, U.e[8].im);
+    }
+};
+
+template <typename T> struct ForceField;
+
+template <> struct ForceField<double> {
+    double2 *p;
+    int Vh;
+    GLAC_HD size_t at(int mu, int par, int k, int s) const {
+        return ((size_t)((mu * 2 + par) * 4 + k)) * (size_t)Vh + (size_t)s;
+    }
+    __device__ __forceinline__ AH8<double> load(int mu, int par, int s) const {
+        AH8<double> Z;
+        double2 v0 = p[at(mu, par, 0, s)], v1 = p[at(mu, par, 1, s)], v2 = p[at(mu, par, 2, s)],
+                v3 = p[at(mu, par, 3, s)];
+        Z.a = v0.x; Z.d = v0.y;
+        Z.b = cx(v1.x, v1.y); Z.c = cx(v2.x, v2.y); Z.e = cx(v3.x, v3.y);
+        return Z;
+    }
+    __device__ __forceinline__ void store(int mu, int par, int s, const AH8<double> &Z) const {
+        p[at(mu, par, 0, s)] = make_double2(Z.a, Z.d);
+        p[at(mu, par, 1, s)] = make_double2(Z.b.re, Z.b.im);
+        p[at(mu, par, 2, s)] = make_double2(Z.c.re, Z.c.im);
+        p[at(mu, par, 3, s)] = make_double2(Z.e.re, Z.e.im);
+    }
+};
+
+template <> struct ForceField<float> {
+    float4 *p;
+    int Vh;
+    GLAC_HD size_t at(int mu, int par, int k, int s) const {
+        return ((size_t)((mu * 2 + par) * 2 + k)) * (size_t)Vh + (size_t)s;
+    }
+    __device__ __forceinline__ AH8<float> load(int mu, int par, int s) const {
+        AH8<float> Z;
+        float4 v0 = p[at(mu, par, 0, s)], v1 = p[at(mu, par, 1, s)];
+        Z.a = v0.x; Z.d = v0.y; Z.b = cx(v0.z, v0.w);
+        Z.c = cx(v1.x, v1.y); Z.e = cx(v1.z, v1.w);
+        return Z;
+    }
+    __device__ __forceinline__ void store(int mu, int par, int s, const AH8<float> &Z) const {
+        p[at(mu, par, 0, s)] = make_float4(Z.a, Z.d, Z.b.re, Z.b.im);
+        p[at(mu, par, 1, s)] = make_float4(Z.c.re, Z.c.im, Z.e.re, Z.e.im);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11)
+// ---------------------------------------------------------------------------
+struct U4 { uint32_t x, y, z, w; };
+
+GLAC_HD U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+#ifdef __CUDA_ARCH__
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+#else
+        uint64_t p0 = (uint64_t)0xD2511F53u * c.x, p1 = (uint64_t)0xCD9E8D57u * c.z;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+        U4 n;
+        n.x = hi1 ^ c.y ^ k0;
+        n.y = lo1;
+        n.z = hi0 ^ c.w ^ k1;
+        n.w = lo0;
+        c = n;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// uniform in (-1/2, 1/2), never 0
+GLAC_HD double u_sym(uint32_t w) { return ((double)w + 0.5) * 2.3283064365386963e-10 - 0.5; }
+GLAC_HD float u_symf(uint32_t w) { return ((float)(w >> 8) + 0.5f) * 5.9604644775390625e-8f - 0.5f; }
+// uniform in [0,1) with 53 bits
+GLAC_HD double u_53(uint32_t hi, uint32_t lo) {
+    return (double)(((uint64_t)hi << 21) | (lo >> 11)) * 1.1102230246251565e-16;
+}
+
+}  // namespace glac

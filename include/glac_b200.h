@@ -1,0 +1,149 @@
+/*
+ * glac_b200 -- C ABI of the B200 (sm_100a) implementation of GLAC's pure-gauge
+ * SU(3) hot path: Wilson-action Metropolis, Luscher RK3 gradient flow with SU(3)
+ * exponentials, and plaquette / clover energy density / topological charge.
+ *
+ * Plain C: pointers and sizes only.  Every entry point returns a glac_status;
+ * on failure glac_last_error() gives the message.  A context owns one lattice,
+ * its device buffers and one CUDA stream; calls on one context are not
+ * re-entrant.
+ *
+ * Host field layout (every *_links argument): 4 blocks (mu = 0..3) of V SU(3)
+ * matrices, each 18 doubles (re, im; row-major), sites in lexicographic order
+ * x + Nx(y + Ny(z + Nz t)) -- exactly the memory of the reference's
+ * Lattice<SU3>[4] (GLAC/math/lattice.h:23-180, GLAC/parallelization/index.h:32-35).
+ *
+ * Observable vectors (every *obs argument): [plaq, topc, energy, topct[0..Nt-1]],
+ * the normalisation of MasterSamplerTopcXYZ::getObservablesVector
+ * (GLAC/observables/mastersamplertopcxyz.cpp:223-234).
+ */
+#ifndef GLAC_B200_H
+#define GLAC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GLAC_OK = 0,
+    GLAC_ERR_ARG = 1,       /* invalid argument (sizes, parities, options) */
+    GLAC_ERR_CUDA = 2,      /* CUDA runtime error or no usable device */
+    GLAC_ERR_TIMEOUT = 3,   /* a bounded device wait ran out */
+    GLAC_ERR_NONFINITE = 4, /* non-finite value in a field or result */
+    GLAC_ERR_IO = 5,        /* file missing, short or of the wrong size */
+    GLAC_ERR_STATE = 6      /* call out of order (e.g. no field set yet) */
+} glac_status;
+
+typedef enum { GLAC_FP64 = 0, GLAC_FP32 = 1 } glac_precision;
+
+/* Reference expFunc names "morningstar", "luscher", "taylor2", "taylor4"
+ * (GLAC/flow/flow.cpp:75-93). */
+typedef enum { GLAC_EXP_MORNINGSTAR = 0, GLAC_EXP_LUSCHER = 1, GLAC_EXP_TAYLOR2 = 2, GLAC_EXP_TAYLOR4 = 3 } glac_exp;
+
+typedef struct {
+    int dims[4];            /* Nx, Ny, Nz, Nt; each even and >= 4 (NSpatial/NTemporal) */
+    double beta;            /* "beta" */
+    int precision;          /* glac_precision */
+    int n_updates;          /* "NUpdates": Metropolis hits per link */
+    double su3_eps;         /* "SU3Eps": proposal spread */
+    double flow_eps;        /* "flowEpsilon" */
+    int exp_func;           /* glac_exp ("expFunc") */
+    uint64_t seed;          /* Philox key ("metropolisSeed") */
+    uint32_t stream_id;     /* Philox stream (independent chains share a seed) */
+    int reunit_interval;    /* FP32: reunitarise every k sweeps / flow steps (0 = never) */
+    int device;             /* CUDA device ordinal */
+} glac_desc;
+
+typedef struct glac_ctx glac_ctx;
+
+/* ---- lifetime ---------------------------------------------------------- */
+/* Replaces System::latticeSetup's allocation (GLAC/system.cpp:148-177, 193-231). */
+glac_status glac_create(const glac_desc *desc, glac_ctx **out);
+void glac_destroy(glac_ctx *ctx);
+const char *glac_last_error(const glac_ctx *ctx);
+/* Message of the last failure of a call that had no context (create, exp_batch ...). */
+const char *glac_global_error(void);
+/* The context's CUDA stream (cudaStream_t), for callers that time or order work. */
+void *glac_stream(glac_ctx *ctx);
+glac_status glac_sync(glac_ctx *ctx);
+/* Number of kernels this context has launched so far. */
+uint64_t glac_launch_count(const glac_ctx *ctx);
+/* Tuning switches: "pair_kernel" (FP32 flow in packed f32x2 lanes, default 1). */
+glac_status glac_set_option(glac_ctx *ctx, const char *key, long value);
+
+/* ---- field --------------------------------------------------------------- */
+/* Cold start (all links 1) -- System::latticeSetup cold branch (GLAC/system.cpp:216-223). */
+glac_status glac_cold_start(glac_ctx *ctx);
+/* Seeded Haar-random start (replaces the hot start, GLAC/system.cpp:200-214). */
+glac_status glac_hot_start(glac_ctx *ctx, uint64_t seed);
+/* Host <-> device in the reference layout; FP32 contexts convert. */
+glac_status glac_set_links(glac_ctx *ctx, const double *host_links);
+glac_status glac_get_links(glac_ctx *ctx, double *host_links);
+/* Same, from / to device memory in the host layout (no host copy). */
+glac_status glac_set_links_device(glac_ctx *ctx, const double *dev_links);
+glac_status glac_get_links_device(glac_ctx *ctx, double *dev_links);
+/* FP64 Gram-Schmidt projection of every link back onto SU(3). */
+glac_status glac_reunitarize(glac_ctx *ctx);
+/* max over links and entries of |U U^+ - 1|. */
+glac_status glac_unitarity_violation(glac_ctx *ctx, double *out);
+
+/* ---- hot path ------------------------------------------------------------- */
+/* n_sweeps checkerboard Metropolis sweeps (replaces System::update,
+ * GLAC/system.cpp:333-361, with WilsonGaugeAction::computeStaple / getDeltaAction,
+ * GLAC/actions/wilsongaugeaction.cpp:24-53).  *acceptance (may be NULL) receives
+ * the mean acceptance per sweep (accepted / (4 NUpdates V), system.cpp:359). */
+glac_status glac_metropolis(glac_ctx *ctx, int n_sweeps, double *acceptance);
+/* n_steps Luscher RK3 steps of the field in place (replaces Flow::flowField,
+ * GLAC/flow/flow.cpp:43-73).  obs (may be NULL) receives (n_steps + 1)
+ * observable vectors: before the first step and after each, as
+ * System::flowConfiguration measures them (GLAC/system.cpp:471-517). */
+glac_status glac_flow(glac_ctx *ctx, int n_steps, double *obs);
+/* Observables of the current field (replaces MasterSamplerTopcXYZ::calculate,
+ * GLAC/observables/mastersamplertopcxyz.cpp:236-384). */
+glac_status glac_measure(glac_ctx *ctx, double *obs);
+/* One load-and-flow pass from host memory: set the field from host_links, then
+ * glac_flow(n_steps, obs) (System::flowConfigurations, GLAC/system.cpp:570-602). */
+glac_status glac_flow_configuration(glac_ctx *ctx, const double *host_links, int n_steps, double *obs);
+
+/* Mean device time in seconds of each of the three RK3 stage launches over
+ * n_steps flow steps of the current field (CUDA events on the context's
+ * stream); advances the field by n_steps. */
+glac_status glac_flow_stage_times(glac_ctx *ctx, int n_steps, double *seconds3);
+
+/* ---- test exports (parity checks against the reference) ------------------ */
+/* Staples of every link of the current field, host layout (computeStaple). */
+glac_status glac_staples(glac_ctx *ctx, double *host_out);
+/* Flow force Z_mu(n) of every link as full matrices (getActionDerivative,
+ * GLAC/actions/wilsongaugeaction.cpp:55-86). */
+glac_status glac_force(glac_ctx *ctx, double *host_out);
+/* exp of n traceless anti-Hermitian matrices on the device (SU3Exp::exp,
+ * GLAC/math/exponentiation/su3exp.cpp:16-79, or the alternates). */
+glac_status glac_exp_batch(int precision, int exp_func, const double *host_in, long n, double *host_out);
+/* dS = -(beta/3) ReTr[(U' - U) A] for n independent triples
+ * (WilsonGaugeAction::getDeltaAction, GLAC/actions/wilsongaugeaction.cpp:24-27). */
+glac_status glac_delta_s_batch(int precision, double beta, long n, const double *host_U, const double *host_Uprime,
+                               const double *host_A, double *host_out);
+/* Metropolis accept step fed with given proposals X[k][h] and uniforms r[k][h]
+ * for independent links k with staple A[k] (GLAC/system.cpp:340-352);
+ * U is updated in place, accept[k][h] receives the decisions. */
+glac_status glac_accept_fed(int precision, double beta, long n_links, int n_hits, double *host_U,
+                            const double *host_A, const double *host_X, const double *host_r,
+                            unsigned char *host_accept);
+
+/* ---- gauge-field files (GLAC/io/fieldio.cpp) ----------------------------- */
+/* Read a GLAC .bin configuration (per site 4 links x 18 doubles, x fastest;
+ * fieldio.cpp:195-257) or, with chroma != 0, its byte-swapped Chroma variant
+ * (fieldio.cpp:259-330) into the host layout. */
+glac_status glac_read_field(const char *path, const int dims[4], int chroma, double *host_links);
+/* Write host-layout links as a GLAC .bin configuration (fieldio.cpp:61-135). */
+glac_status glac_write_field(const char *path, const int dims[4], const double *host_links);
+/* Message of the last failed glac_read_field / glac_write_field on this thread. */
+const char *glac_io_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,220 @@
+"""Parity of the CUDA path (through the C ABI) against the oracle and the
+reference.  Tolerances: FP64 <= 1e-12 relative, FP32 <= 1e-5 relative (the
+bars of the hot-path specification); accept decisions bit-identical."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from test_oracle import gauge_transform, to_c
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-12, "fp32": 1e-5}
+N4 = (4, 4, 4, 4)
+
+
+@pytest.fixture(scope="module")
+def g():
+    import glac_b200
+    return glac_b200
+
+
+def lattice(g, N, precision, **kw):
+    return g.Lattice(N, precision=precision, **kw)
+
+
+def test_known_answers_on_device(g, fixtures):
+    # dS(U=0, U'=U1, A=UTrace) = -(beta/3) ReTr(U1 UTrace) = -(beta/3)(-21)
+    z = np.zeros(18)
+    for prec in ("fp64", "fp32"):
+        ds = g.delta_s_batch(z, fixtures["U1"], fixtures["UTrace"], 3.0, prec)
+        assert ds[0] == 21.0
+
+
+def test_delta_s_cold_lattice(g):
+    # actiontests.cpp:67-114 through the device staple and dS
+    for prec in ("fp64", "fp32"):
+        with lattice(g, (4, 4, 4, 8), prec) as L:
+            L.cold_start()
+            A = L.staples().reshape(-1, 18)
+            U = L.get_links().reshape(-1, 18)
+            Up = np.zeros_like(U)
+            Up[:, [0, 8, 16]] = 2.0
+            ds = g.delta_s_batch(U, Up, A, 6.0, prec)
+            assert np.max(np.abs(ds + 36.0)) <= 1e-15 if prec == "fp64" else 1e-5
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_staples_and_force_vs_reference(g, golden, oracle, prec):
+    with lattice(g, N4, prec) as L:
+        L.set_links(golden["links"])
+        K = golden["staples"].shape[1]
+        assert rel_err(L.staples()[:, :K], golden["staples"]) < TOL[prec]
+        assert rel_err(L.force()[:, :K], golden["force"]) < TOL[prec]
+        assert rel_err(L.staples(), oracle.staples(N4, golden["links"])) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("kind", ["morningstar", "luscher", "taylor2", "taylor4"])
+def test_exponentials_vs_reference(g, golden, prec, kind):
+    out = g.exp_batch(golden["exp_in"], prec, kind)
+    assert rel_err(out, golden["exp_" + kind]) < TOL[prec]
+
+
+def test_morningstar_extreme_inputs(g, oracle):
+    rng = np.random.default_rng(1)
+    for scale in (1e-6, 1e-3, 1.0, 3.0):
+        H = rng.standard_normal((256, 3, 3)) + 1j * rng.standard_normal((256, 3, 3))
+        Z = (H - np.conj(np.transpose(H, (0, 2, 1)))) * 0.5
+        Z -= np.eye(3) * (np.trace(Z, axis1=1, axis2=2)[:, None, None] / 3)
+        Z *= scale
+        m = np.empty((256, 18))
+        m[:, 0::2], m[:, 1::2] = Z.real.reshape(256, 9), Z.imag.reshape(256, 9)
+        want = oracle.exp(m, 4, 30)  # Taylor-30
+        for prec in ("fp64", "fp32"):
+            assert rel_err(g.exp_batch(m, prec), want) < (1e-13 if prec == "fp64" else 2e-6), (scale, prec)
+    # Z = 0: identity (the reference divides 0/0 there, su3exp.cpp:30-31)
+    e = g.exp_batch(np.zeros((1, 18)))
+    assert np.array_equal(e[0][[0, 8, 16]], [1.0, 1.0, 1.0])
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_flow_and_observables_vs_reference(g, golden, prec):
+    with lattice(g, N4, prec, flow_eps=0.01) as L:
+        L.set_links(golden["links"])
+        obs = L.flow(3)
+        assert rel_err(obs[0], golden["observables"]) < TOL[prec]
+        assert rel_err(obs[3], golden["observables_flow3"]) < TOL[prec]
+        assert rel_err(L.get_links(), golden["flow3"]) < TOL[prec]
+
+
+def test_fp32_scalar_and_packed_flow_agree(g, golden):
+    outs = []
+    for pair in (0, 1):
+        with lattice(g, N4, "fp32", flow_eps=0.01) as L:
+            L.set_option("pair_kernel", pair)
+            L.set_links(golden["links"])
+            L.flow(3, measure=False)
+            outs.append(L.get_links())
+    assert rel_err(outs[0], golden["flow3"]) < 1e-5
+    assert rel_err(outs[1], outs[0]) < 1e-5
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_flow_vs_live_reference_larger(g, oracle, reference, prec):
+    N = (8, 8, 8, 8)
+    reference.configure(8, 8, flow_eps=0.02, nflows=4)
+    links = oracle.haar_field(N, 4242)
+    want = reference.flow(links, 4)
+    with lattice(g, N, prec, flow_eps=0.02) as L:
+        L.set_links(links)
+        obs = L.flow(4)
+        assert rel_err(L.get_links(), want) < TOL[prec] * 10
+        assert rel_err(obs[4], reference.observables(want)) < TOL[prec] * 10
+
+
+@pytest.mark.parametrize("kind", ["luscher", "taylor2", "taylor4"])
+def test_flow_alternate_exponentials(g, oracle, golden, kind):
+    k = {"luscher": 1, "taylor2": 2, "taylor4": 3}[kind]
+    want = oracle.flow(N4, golden["links"], 0.01, 2, k)
+    with lattice(g, N4, "fp64", flow_eps=0.01, exp_func=kind) as L:
+        L.set_links(golden["links"])
+        L.flow(2, measure=False)
+        assert rel_err(L.get_links(), want) < 1e-12
+
+
+def test_accept_decisions_bit_identical(g, golden):
+    U, acc = g.accept_fed(golden["mc_U_before"], golden["mc_staples"], golden["mc_X"], golden["mc_r"], 6.0, "fp64")
+    assert np.array_equal(acc, golden["mc_accept"])
+
+
+def test_accept_decisions_full_reference_sweep(g, oracle, reference):
+    reference.configure(4, 8, beta=6.0, su3eps=0.24, nupdates=10, metropolis_seed=17.0, matrix_seed=19.0)
+    tr = reference.metropolis_trace(oracle.haar_field((4, 4, 4, 8), 3))
+    U, acc = g.accept_fed(tr["U_before"], tr["staples"], tr["X"], tr["r"], 6.0, "fp64")
+    assert np.array_equal(acc, tr["accept"])
+    last = {}
+    for k, (mu, s) in enumerate(tr["order"]):
+        last[(mu, s)] = k
+    final = np.array([U[last[(mu, s)]] for mu in range(4) for s in range(512)]).reshape(4, 512, 18)
+    assert rel_err(final, tr["links"]) < 1e-13
+
+
+def test_checkerboard_sweep_matches_oracle(g, oracle):
+    N = (4, 4, 4, 8)
+    start = oracle.haar_field(N, 7)
+    with lattice(g, N, "fp64", beta=6.0, su3_eps=0.24, n_updates=10, seed=0x1234_5678_9ABC, stream_id=3) as L:
+        L.set_links(start)
+        ref = start
+        total = 0
+        for sweep in range(3):
+            ref, a = oracle.metropolis_sweep(N, ref, 6.0, 0.24, 10, 0x1234_5678_9ABC, 3, sweep)
+            total += a
+        acc = L.metropolis(3)
+        assert abs(acc * 4 * 10 * L.V * 3 - total) < 0.5
+        assert rel_err(L.get_links(), ref) < 1e-12
+
+
+def test_hot_start_matches_oracle(g, oracle):
+    N = (4, 4, 4, 8)
+    for prec in ("fp64", "fp32"):
+        with lattice(g, N, prec) as L:
+            L.hot_start(99)
+            got = L.get_links()
+            assert rel_err(got, oracle.haar_field(N, 99)) < (1e-13 if prec == "fp64" else 1e-6)
+            assert L.unitarity_violation() < (1e-13 if prec == "fp64" else 1e-6)
+
+
+def test_set_get_roundtrip(g, oracle):
+    N = (4, 6, 4, 8)
+    links = oracle.haar_field(N, 5)
+    with lattice(g, N, "fp64") as L:
+        L.set_links(links)
+        assert np.array_equal(L.get_links(), links)
+    with lattice(g, N, "fp32") as L:
+        L.set_links(links)
+        assert rel_err(L.get_links(), links) < 1e-7
+
+
+def test_cold_lattice_flow_stays_identity(g):
+    # the reference yields NaN here (0/0 in su3exp.cpp:30-31); the device path returns 1
+    with lattice(g, (4, 4, 4, 4), "fp64") as L:
+        L.cold_start()
+        obs = L.flow(2)
+        assert np.all(np.isfinite(obs))
+        assert obs[-1][0] == 1.0
+
+
+def test_state_and_argument_errors(g):
+    with lattice(g, (4, 4, 4, 4), "fp64") as L:
+        with pytest.raises(g.GlacError) as e:
+            L.flow(1)
+        assert e.value.status == g.GLAC_ERR_STATE
+        L.cold_start()
+        with pytest.raises(g.GlacError) as e:
+            L.metropolis(-1)
+        assert e.value.status == g.GLAC_ERR_ARG
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_gauge_invariance_on_device(g, oracle, prec):
+    N = (8, 8, 8, 16)
+    links = oracle.haar_field(N, 10)
+    W = oracle.haar_field(N, 11)[0]
+    gt = gauge_transform(links, W, N)
+    with lattice(g, N, prec) as L:
+        L.set_links(links)
+        a = L.measure()
+        L.set_links(gt)
+        b = L.measure()
+    assert rel_err(b[:3], a[:3]) < (1e-12 if prec == "fp64" else 1e-5)
+
+
+def test_uneven_extents_and_obs_plan(g, oracle):
+    # Nx != Ny != Nz and half-slices that are not whole warps (6*4*6/2 = 72 sites)
+    N = (6, 4, 6, 4)
+    links = oracle.haar_field(N, 12)
+    with lattice(g, N, "fp64") as L:
+        L.set_links(links)
+        assert rel_err(L.measure(), oracle.observables(N, links)) < 1e-12
+        assert rel_err(L.staples(), oracle.staples(N, links)) < 1e-12
