@@ -352,6 +352,41 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_profile(args):
+    """Small fixed workload for ncu captures and variant timing: hot start, then
+    --steps RK3 steps (with per-step observables unless --no-obs) of one lattice."""
+    import torch
+    import glac_b200 as g
+    dims = tuple(int(x) for x in args.dims.split(","))
+    L = g.Lattice(dims, beta=BETA, precision=args.precision, flow_eps=FLOW_EPS, seed=5, device=0)
+    if args.variant:
+        L.set_option("pair_kernel", 1 if args.variant == "pair" else 0)
+    L.hot_start(7)
+    if args.profile == "metropolis":
+        L.metropolis(args.steps)
+    else:
+        L.flow(args.steps, measure=not args.no_obs)
+    L.sync()
+    V = int(np.prod(dims))
+    if args.time_reps:
+        st = torch.cuda.ExternalStream(L.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        if args.profile == "metropolis":
+            L.metropolis(args.time_reps)
+        else:
+            L.flow(args.time_reps, measure=not args.no_obs)
+        e1.record(st)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3 / args.time_reps
+        stages = L.flow_stage_times(5) if args.profile == "flow" else None
+        print(json.dumps({"profile": args.profile, "dims": dims, "precision": args.precision,
+                          "variant": args.variant, "ms_per_step": sec * 1e3,
+                          "rate": (4 * V if args.profile == "metropolis" else V) / sec,
+                          "stage_ms": None if stages is None else [x * 1e3 for x in stages]}))
+    L.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -360,7 +395,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=25)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", choices=["flow", "metropolis"], help="small workload for ncu / variant timing")
+    ap.add_argument("--dims", default="32,32,32,64")
+    ap.add_argument("--precision", default="fp32")
+    ap.add_argument("--variant", default="", choices=["", "pair", "scalar"])
+    ap.add_argument("--no-obs", action="store_true")
+    ap.add_argument("--time-reps", type=int, default=0)
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
