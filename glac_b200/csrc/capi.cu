@@ -49,36 +49,44 @@ void ck(cudaError_t e, const char *what) {
 }
 void ck_launch(const char *what) { ck(cudaGetLastError(), what); }
 
+// 8 planes of Vh32 tiled sites (see lattice.cuh); FP32 adds the plain float2 plane array.
 size_t field_bytes(const glac_desc &d, const Geom &g) {
-    return (size_t)g.V * 4 * 18 * (d.precision == GLAC_FP64 ? sizeof(double) : sizeof(float));
+    const size_t vh32 = (size_t)round32(g.Vh);
+    if (d.precision == GLAC_FP64) return 8 * vh32 * 9 * sizeof(double2);
+    return 8 * vh32 * 4 * sizeof(float4) + 8 * (size_t)g.Vh * sizeof(float2);
 }
 size_t force_bytes(const glac_desc &d, const Geom &g) {
-    return (size_t)g.V * 4 * 8 * (d.precision == GLAC_FP64 ? sizeof(double) : sizeof(float));
+    const size_t vh32 = (size_t)round32(g.Vh);
+    return d.precision == GLAC_FP64 ? 8 * vh32 * 4 * sizeof(double2) : 8 * vh32 * 2 * sizeof(float4);
 }
 
 LinkField<double> f64(glac_ctx *c, int i) {
     LinkField<double> L;
     L.p = reinterpret_cast<double2 *>(c->field[i]);
     L.Vh = c->g.Vh;
+    L.Vh32 = round32(c->g.Vh);
     return L;
 }
 LinkField<float> f32(glac_ctx *c, int i) {
     LinkField<float> L;
-    L.p4 = reinterpret_cast<float4 *>(c->field[i]);
-    L.p2 = reinterpret_cast<float2 *>(L.p4 + (size_t)16 * c->g.V);
     L.Vh = c->g.Vh;
+    L.Vh32 = round32(c->g.Vh);
+    L.p4 = reinterpret_cast<float4 *>(c->field[i]);
+    L.p2 = reinterpret_cast<float2 *>(L.p4 + (size_t)8 * 4 * L.Vh32);
     return L;
 }
 ForceField<double> z64(glac_ctx *c) {
     ForceField<double> Z;
     Z.p = reinterpret_cast<double2 *>(c->force);
     Z.Vh = c->g.Vh;
+    Z.Vh32 = round32(c->g.Vh);
     return Z;
 }
 ForceField<float> z32(glac_ctx *c) {
     ForceField<float> Z;
     Z.p = reinterpret_cast<float4 *>(c->force);
     Z.Vh = c->g.Vh;
+    Z.Vh32 = round32(c->g.Vh);
     return Z;
 }
 

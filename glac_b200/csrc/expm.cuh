@@ -3,10 +3,15 @@
 // Default: Morningstar-Peardon Cayley-Hamilton form (hep-lat/0311018), the
 // reference's "morningstar" (GLAC/math/exponentiation/su3exp.cpp:16-79).
 // With Q = -i Z (Hermitian, traceless), exp(Z) = exp(iQ) = f0 + f1 Q + f2 Q^2,
-// c0 = det Q = Tr(Q^3)/3, c1 = Tr(Q^2)/2.  The scalar coefficients f_j are
-// always evaluated in FP64 -- also on the FP32 path, where the matrix algebra
-// stays in FP32; this keeps the near-degenerate region (theta -> 0, where acos
-// is ill-conditioned, and small |Q|, where the h_j cancel) accurate.
+// c0 = det Q = Tr(Q^3)/3, c1 = Tr(Q^2)/2.  The coefficients f_j(c0, c1) are
+// evaluated two ways:
+//  * c1 < 0.1 (spectral radius < 0.37, every flow step at eps <= 0.05): the
+//    power series of exp(iQ) reduced by Cayley-Hamilton, Q^3 = c1 Q + c0 1,
+//    in the working precision (16 terms FP64, 9 terms FP32).  It has no
+//    cancellation at small |Q| and no conditioning problem at degenerate
+//    eigenvalues, where the closed form's acos and h_j lose digits.
+//  * otherwise: the closed form of su3exp.cpp:28-76, always in FP64 (also on
+//    the FP32 path, whose matrix algebra stays FP32).
 // Alternates selectable by the run-config's expFunc: "luscher"
 // (expluscher.cpp:13-68), "taylor2" (taylor2exp.cpp:8-16), "taylor4"
 // (taylor4exp.cpp:8-20).
@@ -105,40 +110,87 @@ template <typename R> GLAC_HD HQ2<R> herm_square(const HQ<R> &Q) {
     return S;
 }
 
-// c1 = Tr(Q^2)/2 and c0 = Tr(Q Q^2)/3 evaluated in FP64.
-GLAC_HD void ms_invariants(double q0, double q1, double q2, double xr, double xi, double yr, double yi, double zr,
-                           double zi, double s0, double s1, double s2, double sxr, double sxi, double syr,
-                           double syi, double szr, double szi, double &c0, double &c1) {
-    c1 = 0.5 * (s0 + s1 + s2);
-    // Tr(Q S) = sum_i q_i s_i + 2 Re(x conj(Sx) + y conj(Sy) + z conj(Sz))
-    double t = q0 * s0 + q1 * s1 + q2 * s2;
-    t += 2.0 * (xr * sxr + xi * sxi + yr * syr + yi * syi + zr * szr + zi * szi);
-    c0 = t * 0.3333333333333333;
+// c0 = Tr(Q Q^2)/3 = det Q and c1 = Tr(Q^2)/2 in the working precision.
+template <typename R> GLAC_HD void invariants(const HQ<R> &Q, const HQ2<R> &S, R &c0, R &c1) {
+    c1 = R(0.5f) * (S.d0 + S.d1 + S.d2);
+    R t = Q.q0 * S.d0;
+    t = fmaR(Q.q1, S.d1, t);
+    t = fmaR(Q.q2, S.d2, t);
+    R o = Q.x.re * S.x.re;
+    o = fmaR(Q.x.im, S.x.im, o);
+    o = fmaR(Q.y.re, S.y.re, o);
+    o = fmaR(Q.y.im, S.y.im, o);
+    o = fmaR(Q.z.re, S.z.re, o);
+    o = fmaR(Q.z.im, S.z.im, o);
+    c0 = (t + o + o) * R(0.33333333333333333);
+}
+template <> GLAC_HD void invariants<f32x2>(const HQ<f32x2> &Q, const HQ2<f32x2> &S, f32x2 &c0, f32x2 &c1) {
+    c1 = f32x2(0.5f) * (S.d0 + S.d1 + S.d2);
+    f32x2 t = Q.q0 * S.d0;
+    t = fmaR(Q.q1, S.d1, t);
+    t = fmaR(Q.q2, S.d2, t);
+    f32x2 o = Q.x.re * S.x.re;
+    o = fmaR(Q.x.im, S.x.im, o);
+    o = fmaR(Q.y.re, S.y.re, o);
+    o = fmaR(Q.y.im, S.y.im, o);
+    o = fmaR(Q.z.re, S.z.re, o);
+    o = fmaR(Q.z.im, S.z.im, o);
+    c0 = (t + o + o) * f32x2(0.33333334f);
 }
 
-template <typename R> GLAC_HD ExpCoef coef_of(const HQ<R> &Q, const HQ2<R> &S);
-template <> GLAC_HD ExpCoef coef_of<double>(const HQ<double> &Q, const HQ2<double> &S) {
-    double c0, c1;
-    ms_invariants(Q.q0, Q.q1, Q.q2, Q.x.re, Q.x.im, Q.y.re, Q.y.im, Q.z.re, Q.z.im, S.d0, S.d1, S.d2, S.x.re,
-                  S.x.im, S.y.re, S.y.im, S.z.re, S.z.im, c0, c1);
-    return ms_coefficients(c0, c1);
+template <typename R> struct SeriesTerms { static const int n = 9; };
+template <> struct SeriesTerms<double> { static const int n = 16; };
+#define GLAC_SERIES_C1_MAX 0.1
+
+// exp(iQ) = sum_n i^n Q^n / n!,  Q^n = a_n 1 + b_n Q + g_n Q^2 with
+// a_{n+1} = c0 g_n, b_{n+1} = a_n + c1 g_n, g_{n+1} = b_n  (a, b, g carry 1/n!).
+template <typename R> GLAC_HD void ms_series(R c0, R c1, Cx<R> &f0, Cx<R> &f1, Cx<R> &f2) {
+    R a = R(1.f), b = rzero<R>(), gg = rzero<R>();
+    R z = rzero<R>();
+    f0 = cx(z, z); f1 = cx(z, z); f2 = cx(z, z);
+#pragma unroll
+    for (int n = 0; n < SeriesTerms<R>::n; n++) {
+        switch (n & 3) {
+        case 0: f0.re = f0.re + a; f1.re = f1.re + b; f2.re = f2.re + gg; break;
+        case 1: f0.im = f0.im + a; f1.im = f1.im + b; f2.im = f2.im + gg; break;
+        case 2: f0.re = f0.re - a; f1.re = f1.re - b; f2.re = f2.re - gg; break;
+        default: f0.im = f0.im - a; f1.im = f1.im - b; f2.im = f2.im - gg; break;
+        }
+        const R inv = R(1.0f / (float)(n + 1));
+        const R a1 = c0 * gg * inv;
+        const R b1 = fmaR(c1, gg, a) * inv;
+        gg = b * inv;
+        a = a1;
+        b = b1;
+    }
 }
-template <> GLAC_HD ExpCoef coef_of<float>(const HQ<float> &Q, const HQ2<float> &S) {
-    double c0, c1;
-    ms_invariants(Q.q0, Q.q1, Q.q2, Q.x.re, Q.x.im, Q.y.re, Q.y.im, Q.z.re, Q.z.im, S.d0, S.d1, S.d2, S.x.re,
-                  S.x.im, S.y.re, S.y.im, S.z.re, S.z.im, c0, c1);
-    return ms_coefficients(c0, c1);
+template <> GLAC_HD void ms_series<double>(double c0, double c1, Cx<double> &f0, Cx<double> &f1, Cx<double> &f2) {
+    double a = 1.0, b = 0.0, gg = 0.0;
+    f0 = cx(0.0, 0.0); f1 = cx(0.0, 0.0); f2 = cx(0.0, 0.0);
+#pragma unroll
+    for (int n = 0; n < SeriesTerms<double>::n; n++) {
+        switch (n & 3) {
+        case 0: f0.re += a; f1.re += b; f2.re += gg; break;
+        case 1: f0.im += a; f1.im += b; f2.im += gg; break;
+        case 2: f0.re -= a; f1.re -= b; f2.re -= gg; break;
+        default: f0.im -= a; f1.im -= b; f2.im -= gg; break;
+        }
+        const double inv = 1.0 / (double)(n + 1);
+        const double a1 = c0 * gg * inv;
+        const double b1 = fma(c1, gg, a) * inv;
+        gg = b * inv;
+        a = a1;
+        b = b1;
+    }
 }
 
 template <typename R> GLAC_HD R from_d(double v);
 template <> GLAC_HD double from_d<double>(double v) { return v; }
 template <> GLAC_HD float from_d<float>(double v) { return (float)v; }
 
-// exp(Z) as a full matrix (f0 + f1 Q + f2 Q^2).
-template <typename R> GLAC_HD M3<R> ms_expm_from(const HQ<R> &Q, const HQ2<R> &S, const ExpCoef &f) {
-    Cx<R> f0 = cx(from_d<R>(f.f0r), from_d<R>(f.f0i));
-    Cx<R> f1 = cx(from_d<R>(f.f1r), from_d<R>(f.f1i));
-    Cx<R> f2 = cx(from_d<R>(f.f2r), from_d<R>(f.f2i));
+// f0 + f1 Q + f2 Q^2 as a full matrix.
+template <typename R>
+GLAC_HD M3<R> ms_combine(const HQ<R> &Q, const HQ2<R> &S, Cx<R> f0, Cx<R> f1, Cx<R> f2) {
     M3<R> E;
     // diagonal: f0 + f1 q_i + f2 s_i  (q_i, s_i real)
     E(0, 0) = cx(fmaR(f1.re, Q.q0, fmaR(f2.re, S.d0, f0.re)), fmaR(f1.im, Q.q0, fmaR(f2.im, S.d0, f0.im)));
@@ -155,38 +207,40 @@ template <typename R> GLAC_HD M3<R> ms_expm_from(const HQ<R> &Q, const HQ2<R> &S
 }
 
 template <typename R> GLAC_HD M3<R> expm_morningstar(const AH8<R> &Z) {
-    HQ<R> Q = herm_from_ah(Z);
-    HQ2<R> S = herm_square(Q);
-    ExpCoef f = coef_of(Q, S);
-    return ms_expm_from(Q, S, f);
+    const HQ<R> Q = herm_from_ah(Z);
+    const HQ2<R> S = herm_square(Q);
+    R c0, c1;
+    invariants(Q, S, c0, c1);
+    Cx<R> f0, f1, f2;
+    if (c1 < R(GLAC_SERIES_C1_MAX)) {
+        ms_series(c0, c1, f0, f1, f2);
+    } else {
+        const ExpCoef f = ms_coefficients((double)c0, (double)c1);
+        f0 = cx(from_d<R>(f.f0r), from_d<R>(f.f0i));
+        f1 = cx(from_d<R>(f.f1r), from_d<R>(f.f1i));
+        f2 = cx(from_d<R>(f.f2r), from_d<R>(f.f2i));
+    }
+    return ms_combine(Q, S, f0, f1, f2);
 }
 
-// Packed pair: coefficients per lane in FP64, matrix algebra in packed FP32.
+// Packed pair: the series in packed FP32 lanes; the FP64 closed form per lane
+// only when a lane leaves the series range.
 GLAC_HD M3<f32x2> expm_morningstar_pair(const AH8<f32x2> &Z) {
-    HQ<f32x2> Q = herm_from_ah(Z);
-    HQ2<f32x2> S = herm_square(Q);
-    double c0x, c1x, c0y, c1y;
-    ms_invariants(Q.q0.v.x, Q.q1.v.x, Q.q2.v.x, Q.x.re.v.x, Q.x.im.v.x, Q.y.re.v.x, Q.y.im.v.x, Q.z.re.v.x,
-                  Q.z.im.v.x, S.d0.v.x, S.d1.v.x, S.d2.v.x, S.x.re.v.x, S.x.im.v.x, S.y.re.v.x, S.y.im.v.x,
-                  S.z.re.v.x, S.z.im.v.x, c0x, c1x);
-    ms_invariants(Q.q0.v.y, Q.q1.v.y, Q.q2.v.y, Q.x.re.v.y, Q.x.im.v.y, Q.y.re.v.y, Q.y.im.v.y, Q.z.re.v.y,
-                  Q.z.im.v.y, S.d0.v.y, S.d1.v.y, S.d2.v.y, S.x.re.v.y, S.x.im.v.y, S.y.re.v.y, S.y.im.v.y,
-                  S.z.re.v.y, S.z.im.v.y, c0y, c1y);
-    ExpCoef a = ms_coefficients(c0x, c1x), b = ms_coefficients(c0y, c1y);
-    Cx<f32x2> f0 = cx(f32x2((float)a.f0r, (float)b.f0r), f32x2((float)a.f0i, (float)b.f0i));
-    Cx<f32x2> f1 = cx(f32x2((float)a.f1r, (float)b.f1r), f32x2((float)a.f1i, (float)b.f1i));
-    Cx<f32x2> f2 = cx(f32x2((float)a.f2r, (float)b.f2r), f32x2((float)a.f2i, (float)b.f2i));
-    M3<f32x2> E;
-    E(0, 0) = cx(fmaR(f1.re, Q.q0, fmaR(f2.re, S.d0, f0.re)), fmaR(f1.im, Q.q0, fmaR(f2.im, S.d0, f0.im)));
-    E(1, 1) = cx(fmaR(f1.re, Q.q1, fmaR(f2.re, S.d1, f0.re)), fmaR(f1.im, Q.q1, fmaR(f2.im, S.d1, f0.im)));
-    E(2, 2) = cx(fmaR(f1.re, Q.q2, fmaR(f2.re, S.d2, f0.re)), fmaR(f1.im, Q.q2, fmaR(f2.im, S.d2, f0.im)));
-    E(0, 1) = cmac(f1 * Q.x, f2, S.x);
-    E(1, 0) = cmac(f1 * conj(Q.x), f2, conj(S.x));
-    E(0, 2) = cmac(f1 * Q.y, f2, S.y);
-    E(2, 0) = cmac(f1 * conj(Q.y), f2, conj(S.y));
-    E(1, 2) = cmac(f1 * Q.z, f2, S.z);
-    E(2, 1) = cmac(f1 * conj(Q.z), f2, conj(S.z));
-    return E;
+    const HQ<f32x2> Q = herm_from_ah(Z);
+    const HQ2<f32x2> S = herm_square(Q);
+    f32x2 c0, c1;
+    invariants(Q, S, c0, c1);
+    Cx<f32x2> f0, f1, f2;
+    if (c1.v.x < (float)GLAC_SERIES_C1_MAX && c1.v.y < (float)GLAC_SERIES_C1_MAX) {
+        ms_series(c0, c1, f0, f1, f2);
+    } else {
+        const ExpCoef a = ms_coefficients((double)c0.v.x, (double)c1.v.x);
+        const ExpCoef b = ms_coefficients((double)c0.v.y, (double)c1.v.y);
+        f0 = cx(f32x2((float)a.f0r, (float)b.f0r), f32x2((float)a.f0i, (float)b.f0i));
+        f1 = cx(f32x2((float)a.f1r, (float)b.f1r), f32x2((float)a.f1i, (float)b.f1i));
+        f2 = cx(f32x2((float)a.f2r, (float)b.f2r), f32x2((float)a.f2i, (float)b.f2i));
+    }
+    return ms_combine(Q, S, f0, f1, f2);
 }
 
 // ---------------------------------------------------------------------------

@@ -8,6 +8,10 @@
 
 namespace glac {
 
+// Minimum resident blocks per SM requested from ptxas (caps registers per thread).
+template <typename T> struct MinBlocks { static const int obs = 1, metro = 4, flow = 4; };
+template <> struct MinBlocks<double> { static const int obs = 1, metro = 3, flow = 3; };
+
 // ---------------------------------------------------------------------------
 // Flow stage (GLAC/flow/flow.cpp:43-73 with getActionDerivative,
 // GLAC/actions/wilsongaugeaction.cpp:55-86), one fused pass per RK3 stage:
@@ -16,14 +20,17 @@ namespace glac {
 //   stage 1: M = (8/9 eps) Z1 - (17/36 eps) Z0, stores M
 //   stage 2: M = (3/4 eps) Z2 - M_prev
 // Reads field `in`, writes `out` (all four Z_mu come from the same field).
-// grid: x over the Vh sites of a parity plane, y = mu*2 + parity.
+// 1-D grid, the 8 (mu, parity) planes interleaved fastest: the blocks that run
+// together cover one region of the lattice for all planes, so the neighbour
+// links they share are read from HBM once and then hit in L2.
 // ---------------------------------------------------------------------------
 template <typename T, int KIND, int STAGE>
 __global__ void __launch_bounds__(128) k_flow_stage(Geom g, LinkField<T> in, LinkField<T> out, ForceField<T> zf,
                                                     T alpha, T beta) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int plane = blockIdx.x & 7;
+    const int s = (blockIdx.x >> 3) * blockDim.x + threadIdx.x;
     if (s >= g.Vh) return;
-    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    const int mu = plane >> 1, p = plane & 1;
     const Site n = site_from_ps(g, p, s);
     M3<T> A = staple(in, g, n, p, mu);
     const M3<T> U = in.load(mu, p, s);
@@ -44,7 +51,7 @@ template <typename T>
 void launch_flow_stage(const Geom &g, const LinkField<T> &in, const LinkField<T> &out, const ForceField<T> &zf,
                        int stage, int kind, double alpha, double beta, int block, cudaStream_t st) {
     (void)block;
-    dim3 grid((g.Vh + 127) / 128, 8);
+    dim3 grid(8 * ((g.Vh + 127) / 128));
     T a = (T)alpha, b = (T)beta;
 #define GLAC_FLOW_CASE(K, S) \
     if (kind == K && stage == S) { k_flow_stage<T, K, S><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); return; }
@@ -129,11 +136,12 @@ __device__ __forceinline__ M3<f32x2> staple_pair(const LinkField<float> &L, cons
 template <int STAGE>
 __global__ void __launch_bounds__(128) k_flow_stage_pair(Geom g, LinkField<float> in, LinkField<float> out,
                                                          ForceField<float> zf, float alpha, float beta) {
-    const int s0 = blockIdx.x * (2 * blockDim.x) + threadIdx.x;
+    const int plane = blockIdx.x & 7;
+    const int s0 = (blockIdx.x >> 3) * (2 * blockDim.x) + threadIdx.x;
     if (s0 >= g.Vh) return;
     const bool has1 = s0 + (int)blockDim.x < g.Vh;
     const int s1 = has1 ? s0 + (int)blockDim.x : s0;
-    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    const int mu = plane >> 1, p = plane & 1;
     const Site n0 = site_from_ps(g, p, s0), n1 = site_from_ps(g, p, s1);
     M3<f32x2> A = staple_pair(in, g, n0, n1, p, mu);
     const M3<f32x2> U = pack2(in.load(mu, p, s0), in.load(mu, p, s1));
@@ -165,7 +173,7 @@ void launch_flow_stage_pair(const Geom &g, const LinkField<float> &in, const Lin
                             const ForceField<float> &zf, int stage, double alpha, double beta, int block,
                             cudaStream_t st) {
     (void)block;
-    dim3 grid((g.Vh + 255) / 256, 8);
+    dim3 grid(8 * ((g.Vh + 255) / 256));
     float a = (float)alpha, b = (float)beta;
     if (stage == 0) k_flow_stage_pair<0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b);
     else if (stage == 1) k_flow_stage_pair<1><<<grid, 128, 0, st>>>(g, in, out, zf, a, b);
@@ -174,18 +182,24 @@ void launch_flow_stage_pair(const Geom &g, const LinkField<float> &in, const Lin
 
 // ---------------------------------------------------------------------------
 // Checkerboard Metropolis sub-sweep over the links (mu, parity p).
-// Staple once per link, then nhits proposals U' = X U with X = R S T or its
+// Staple A once per link, then nhits proposals U' = X U with X = R S T or its
 // inverse (GLAC/math/matrices/su3matrixgenerator.h:170-321), accepted iff
 // exp(-dS) > r with dS = -(beta/3) ReTr[(U' - U) A] (GLAC/system.cpp:333-361,
 // GLAC/actions/wilsongaugeaction.cpp:24-27).  The links of one (mu, parity)
 // class do not enter each other's staples, so they update concurrently.
-// Random numbers: Philox4x32-10, key = seed, counter = {4 hit + call,
-// mu V + lex, sweep, stream}; words 0-11 build R, S, T, word 12 picks X or
-// X^+, words 13-14 give the 53-bit accept uniform.
+// Each hit needs only ReTr(X W) with W = U A kept up to date, since
+// ReTr[(XU - U) A] = ReTr(X W) - ReTr(W); the products X U and X W are formed
+// only for accepted proposals.
+// Random numbers: Philox4x32-10, key = seed, counter = {2 hit + call,
+// mu V + lex, sweep, stream}: words 0-5 carry twelve 16-bit uniforms (low half
+// first) for R, S, T; words 6-7 the 53-bit accept uniform; bit 0 of word 7
+// picks X or X^+.
 // ---------------------------------------------------------------------------
 template <typename T> __device__ __forceinline__ T su_scalar(double v);
 template <> __device__ __forceinline__ double su_scalar<double>(double v) { return v; }
 template <> __device__ __forceinline__ float su_scalar<float>(double v) { return (float)v; }
+
+GLAC_HD double u_sym16(uint32_t h) { return ((double)h + 0.5) * (1.0 / 65536.0) - 0.5; }
 
 template <typename T>
 __device__ __forceinline__ void su2_near_unity(T u0, T u1, T u2, T u3, T eps, T sq1me, T out[4]) {
@@ -198,39 +212,52 @@ __device__ __forceinline__ void su2_near_unity(T u0, T u1, T u2, T u3, T eps, T 
     out[0] = x0 / nrm; out[1] = x1 / nrm; out[2] = x2 / nrm; out[3] = x3 / nrm;
 }
 
-// X = R S T with R, S, T the SU(2) elements [[x0 + i x3, x2 + i x1], [-x2 + i x1, x0 - i x3]]
-// embedded in the (12), (13), (23) blocks; inverse -> X^+.
+// X = R S T with the SU(2) elements [[x0 + i x3, x2 + i x1], [-x2 + i x1, x0 - i x3]]
+// embedded in the (12), (13), (23) blocks; zero blocks skipped.  inverse -> X^+.
 template <typename T>
 __device__ __forceinline__ M3<T> rst_matrix(const T r[4], const T s[4], const T t[4], bool inverse) {
-    M3<T> R, S, Tm;
-    set_zero(R); set_zero(S); set_zero(Tm);
-    R(0, 0) = cx(r[0], r[3]); R(0, 1) = cx(r[2], r[1]); R(1, 0) = cx(-r[2], r[1]); R(1, 1) = cx(r[0], -r[3]);
-    R(2, 2).re = T(1);
-    S(0, 0) = cx(s[0], s[3]); S(0, 2) = cx(s[2], s[1]); S(2, 0) = cx(-s[2], s[1]); S(2, 2) = cx(s[0], -s[3]);
-    S(1, 1).re = T(1);
-    Tm(1, 1) = cx(t[0], t[3]); Tm(1, 2) = cx(t[2], t[1]); Tm(2, 1) = cx(-t[2], t[1]); Tm(2, 2) = cx(t[0], -t[3]);
-    Tm(0, 0).re = T(1);
-    M3<T> X = mul(mul(R, S), Tm);
+    const Cx<T> r00 = cx(r[0], r[3]), r01 = cx(r[2], r[1]), r10 = cx(-r[2], r[1]), r11 = cx(r[0], -r[3]);
+    const Cx<T> s00 = cx(s[0], s[3]), s01 = cx(s[2], s[1]), s10 = cx(-s[2], s[1]), s11 = cx(s[0], -s[3]);
+    const Cx<T> t00 = cx(t[0], t[3]), t01 = cx(t[2], t[1]), t10 = cx(-t[2], t[1]), t11 = cx(t[0], -t[3]);
+    // R S = [[r00 s00, r01, r00 s01], [r10 s00, r11, r10 s01], [s10, 0, s11]]
+    const Cx<T> a0 = r00 * s00, a2 = r00 * s01, b0 = r10 * s00, b2 = r10 * s01;
+    M3<T> X;
+    X(0, 0) = a0;
+    X(1, 0) = b0;
+    X(2, 0) = s10;
+    X(0, 1) = cmac(r01 * t00, a2, t10);
+    X(1, 1) = cmac(r11 * t00, b2, t10);
+    X(2, 1) = s11 * t10;
+    X(0, 2) = cmac(r01 * t01, a2, t11);
+    X(1, 2) = cmac(r11 * t01, b2, t11);
+    X(2, 2) = s11 * t11;
     return inverse ? dagger(X) : X;
 }
 
 template <typename T>
 __device__ __forceinline__ void draw_proposal(uint32_t k0, uint32_t k1, uint32_t link_id, uint32_t sweep,
                                               uint32_t stream_id, int hit, T eps, T sq1me, M3<T> &X, double &r) {
-    uint32_t w[16];
+    uint32_t w[8];
 #pragma unroll
-    for (int call = 0; call < 4; call++) {
-        U4 c = {(uint32_t)(4 * hit + call), link_id, sweep, stream_id};
+    for (int call = 0; call < 2; call++) {
+        U4 c = {(uint32_t)(2 * hit + call), link_id, sweep, stream_id};
         U4 o = philox4x32_10(c, k0, k1);
         w[4 * call] = o.x; w[4 * call + 1] = o.y; w[4 * call + 2] = o.z; w[4 * call + 3] = o.w;
     }
     T su[3][4];
 #pragma unroll
-    for (int b = 0; b < 3; b++)
-        su2_near_unity<T>(su_scalar<T>(u_sym(w[4 * b])), su_scalar<T>(u_sym(w[4 * b + 1])),
-                          su_scalar<T>(u_sym(w[4 * b + 2])), su_scalar<T>(u_sym(w[4 * b + 3])), eps, sq1me, su[b]);
-    X = rst_matrix<T>(su[0], su[1], su[2], (w[12] & 0x80000000u) == 0u);
-    r = u_53(w[13], w[14]);
+    for (int b = 0; b < 3; b++) {
+        T u[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int k = 4 * b + c;
+            const uint32_t word = w[k >> 1];
+            u[c] = su_scalar<T>(u_sym16((k & 1) ? (word >> 16) : (word & 0xFFFFu)));
+        }
+        su2_near_unity<T>(u[0], u[1], u[2], u[3], eps, sq1me, su[b]);
+    }
+    X = rst_matrix<T>(su[0], su[1], su[2], (w[7] & 1u) == 0u);
+    r = u_53(w[6], w[7]);
 }
 
 template <typename T> __device__ __forceinline__ double accept_weight(T dS);
@@ -261,7 +288,7 @@ __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned lon
 }
 
 template <typename T>
-__global__ void __launch_bounds__(128) k_metropolis(Geom g, LinkField<T> L, int mu, int p, T mfac, T eps, T sq1me,
+__global__ void __launch_bounds__(128, MinBlocks<T>::metro) k_metropolis(Geom g, LinkField<T> L, int mu, int p, T mfac, T eps, T sq1me,
                                                     int nhits, uint32_t k0, uint32_t k1, uint32_t sweep,
                                                     uint32_t stream_id, unsigned long long *acc) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -270,15 +297,17 @@ __global__ void __launch_bounds__(128) k_metropolis(Geom g, LinkField<T> L, int 
         const Site n = site_from_ps(g, p, s);
         const M3<T> A = staple(L, g, n, p, mu);
         M3<T> U = L.load_rw(mu, p, s);
+        M3<T> W = mul(U, A);
         const uint32_t link_id = (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex;
 #pragma unroll 1
         for (int h = 0; h < nhits; h++) {
             M3<T> X;
             double r;
             draw_proposal<T>(k0, k1, link_id, sweep, stream_id, h, eps, sq1me, X, r);
-            const M3<T> Up = mul(X, U);
-            if (accept_weight<T>(delta_s(U, Up, A, mfac)) > r) {
-                U = Up;
+            const T dS = (retr_mul(X, W) - retr(W)) * mfac;
+            if (accept_weight<T>(dS) > r) {
+                U = mul(X, U);
+                W = mul(X, W);
                 na++;
             }
         }
@@ -326,9 +355,12 @@ ObsPlan make_obs_plan(const Geom &g) {
     return pl;
 }
 
+// Clover of the (mu, nu) plane at n, projected: F = (C - C^+) - 1/3 i ImTr(C - C^+),
+// returned in the 8-real form; *plaq = ReTr(leaf1).  Links are re-read from
+// L1/L2 rather than held, to keep register pressure low.
 template <typename T>
-__device__ __forceinline__ void clover(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu, int nu,
-                                       M3<T> &C, T &plaq) {
+__device__ __forceinline__ AH8<T> clover_ah(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu,
+                                            int nu, T &plaq) {
     const int q = p ^ 1;
     const int s_n = n.lex >> 1;
     const int s_mup = lex_step(g, n, mu, +1) >> 1;           // n+mu      (q)
@@ -338,41 +370,57 @@ __device__ __forceinline__ void clover(const LinkField<T> &L, const Geom &g, con
     const int s_pm = lex_step2(g, n, mu, +1, nu, -1) >> 1;   // n+mu-nu   (p)
     const int s_mm = lex_step2(g, n, mu, -1, nu, -1) >> 1;   // n-mu-nu   (p)
     const int s_mp = lex_step2(g, n, mu, -1, nu, +1) >> 1;   // n-mu+nu   (p)
-    const M3<T> Umu = L.load(mu, p, s_n);
-    const M3<T> Unu = L.load(nu, p, s_n);
-    // leaf1 = U_mu(n) U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+
-    {
-        M3<T> P = mul(Umu, L.load(nu, q, s_mup));
-        M3<T> W = mul(Unu, L.load(mu, q, s_nup));
+    M3<T> C;
+    // compiler fences between the leaves keep their loads from being hoisted
+    // together, which would multiply the live registers
+    {   // leaf1 = U_mu(n) U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+
+        const M3<T> P = mul(L.load(mu, p, s_n), L.load(nu, q, s_mup));
+        const M3<T> W = mul(L.load(nu, p, s_n), L.load(mu, q, s_nup));
         C = mul_nd(P, W);
         plaq = retr(C);
     }
-    const M3<T> Unu_m = L.load(nu, q, s_num);  // U_nu(n-nu)
-    // leaf2 = U_mu(n) U_nu(n+mu-nu)^+ U_mu(n-nu)^+ U_nu(n-nu)
-    {
-        M3<T> Y = mul(L.load(mu, q, s_num), L.load(nu, p, s_pm));
-        sub_from(C, mul(mul_nd(Umu, Y), Unu_m));
+    asm volatile("" ::: "memory");
+    {   // leaf2 = U_mu(n) U_nu(n+mu-nu)^+ U_mu(n-nu)^+ U_nu(n-nu)
+        const M3<T> Y = mul(L.load(mu, q, s_num), L.load(nu, p, s_pm));
+        const M3<T> t = mul_nd(L.load(mu, p, s_n), Y);
+        sub_from(C, mul(t, L.load(nu, q, s_num)));
     }
-    const M3<T> Umu_m = L.load(mu, q, s_mum);  // U_mu(n-mu)
-    // leaf3 = U_mu(n-mu)^+ U_nu(n-mu-nu)^+ U_mu(n-mu-nu) U_nu(n-nu)
-    {
-        M3<T> t = mul_dd(Umu_m, L.load(nu, p, s_mm));
+    asm volatile("" ::: "memory");
+    {   // leaf3 = U_mu(n-mu)^+ U_nu(n-mu-nu)^+ U_mu(n-mu-nu) U_nu(n-nu)
+        M3<T> t = mul_dd(L.load(mu, q, s_mum), L.load(nu, p, s_mm));
         t = mul(t, L.load(mu, p, s_mm));
-        add_to(C, mul(t, Unu_m));
+        add_to(C, mul(t, L.load(nu, q, s_num)));
     }
-    // leaf4 = U_mu(n-mu)^+ U_nu(n-mu) U_mu(n-mu+nu) U_nu(n)^+
-    {
-        M3<T> t = mul_dn(Umu_m, L.load(nu, q, s_mum));
+    asm volatile("" ::: "memory");
+    {   // leaf4 = U_mu(n-mu)^+ U_nu(n-mu) U_mu(n-mu+nu) U_nu(n)^+
+        M3<T> t = mul_dn(L.load(mu, q, s_mum), L.load(nu, q, s_mum));
         t = mul(t, L.load(mu, p, s_mp));
-        sub_from(C, mul_nd(t, Unu));
+        sub_from(C, mul_nd(t, L.load(nu, p, s_n)));
     }
-    // (C - C^+) - 1/3 i ImTr(C - C^+)
-    M3<T> D = dagger(C);
-    sub_from(C, D);
-    T tr = (C(0, 0).im + C(1, 1).im + C(2, 2).im) / T(3);
-    C(0, 0).im = C(0, 0).im - tr;
-    C(1, 1).im = C(1, 1).im - tr;
-    C(2, 2).im = C(2, 2).im - tr;
+    // (C - C^+): diagonal 2 i Im C_ii, off-diagonal C_ij - conj(C_ji); then traceless
+    AH8<T> F;
+    const T two = T(2);
+    const T tr = (C(0, 0).im + C(1, 1).im + C(2, 2).im) * T(2.0 / 3.0);
+    F.a = two * C(0, 0).im - tr;
+    F.d = two * C(1, 1).im - tr;
+    F.b = cx(C(0, 1).re - C(1, 0).re, C(0, 1).im + C(1, 0).im);
+    F.c = cx(C(0, 2).re - C(2, 0).re, C(0, 2).im + C(2, 0).im);
+    F.e = cx(C(1, 2).re - C(2, 1).re, C(1, 2).im + C(2, 1).im);
+    return F;
+}
+
+// Re Tr(F G) for traceless anti-Hermitian F, G in the 8-real form:
+//   -[a a' + d d' + (a+d)(a'+d')] - 2 Re(b b'* + c c'* + e e'*)
+template <typename T>
+__device__ __forceinline__ T retr_ah(const AH8<T> &F, const AH8<T> &G) {
+    T diag = fmaR(F.a, G.a, F.d * G.d);
+    diag = fmaR(F.a + F.d, G.a + G.d, diag);
+    T off = fmaR(F.b.re, G.b.re, F.b.im * G.b.im);
+    off = fmaR(F.c.re, G.c.re, off);
+    off = fmaR(F.c.im, G.c.im, off);
+    off = fmaR(F.e.re, G.e.re, off);
+    off = fmaR(F.e.im, G.e.im, off);
+    return -(diag + off + off);
 }
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -382,7 +430,7 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_observables(Geom g, LinkField<T> L, int nb, int Bv, double *partial) {
+__global__ void __launch_bounds__(256, MinBlocks<T>::obs) k_observables(Geom g, LinkField<T> L, int nb, int Bv, double *partial) {
     const int b = blockIdx.x;
     const int t = b / (2 * nb);
     const int p = (b / nb) & 1;
@@ -392,16 +440,17 @@ __global__ void __launch_bounds__(256) k_observables(Geom g, LinkField<T> L, int
     const int s = t * half_slice + j * Bv + (valid ? (int)threadIdx.x : 0);
     double plaq = 0.0, en = 0.0, qt = 0.0;
     const Site n = site_from_ps(g, p, s);
+    if (valid) {
 #pragma unroll 1
-    for (int nu = 1; nu < 4 && valid; nu++) {
-        const int rho = nu % 3 + 1, sigma = rho % 3 + 1;
-        M3<T> C1, C2;
-        T pl1, pl2;
-        clover(L, g, n, p, 0, nu, C1, pl1);
-        clover(L, g, n, p, rho, sigma, C2, pl2);
-        plaq += (double)pl1 + (double)pl2;
-        qt -= (double)retr_mul(C1, C2);
-        en += (double)retr_mul(C1, C1) + (double)retr_mul(C2, C2);
+        for (int nu = 1; nu < 4; nu++) {
+            const int rho = nu % 3 + 1, sigma = rho % 3 + 1;
+            T pl1, pl2;
+            const AH8<T> F1 = clover_ah(L, g, n, p, 0, nu, pl1);
+            const AH8<T> F2 = clover_ah(L, g, n, p, rho, sigma, pl2);
+            plaq += (double)pl1 + (double)pl2;
+            qt -= (double)retr_ah(F1, F2);
+            en += (double)retr_ah(F1, F1) + (double)retr_ah(F2, F2);
+        }
     }
     // deterministic block reduction
     __shared__ double sh[3][32];

@@ -1,18 +1,23 @@
 // Lattice geometry, the HBM layout of gauge fields, and the Philox streams.
 //
-// Layout (structure of arrays, even/odd split): a field of 4 link directions
-// over V = Nx Ny Nz Nt sites is stored per (mu, parity) plane of Vh = V/2
-// sites, each link split into 16-byte chunks so that a warp reading 32
-// consecutive sites of one chunk issues fully coalesced 128-bit loads:
-//   FP64: 9 double2 chunks   chunk k = complex element k (row-major)
-//         addr = ((mu*2 + p)*9 + k)*Vh + s
-//   FP32: 4 float4 chunks (complex elements 2k, 2k+1) + 1 float2 chunk (element 8)
-//         addr4 = ((mu*2 + p)*4 + k)*Vh + s ,  addr2 = (mu*2 + p)*Vh + s
+// Layout (even/odd split, arrays of 32-site tiles): a field of 4 link
+// directions over V = Nx Ny Nz Nt sites is stored per (mu, parity) plane of
+// Vh = V/2 sites.  Inside a plane the sites form tiles of 32 (Vh32 = Vh rounded
+// up to 32); a tile holds each 16-byte chunk of its 32 links contiguously, so a
+// warp reading 32 consecutive sites of one chunk issues fully coalesced 128-bit
+// loads, and the chunks of one link sit at fixed 512-byte offsets from one base
+// address (no per-chunk address registers):
+//   FP64: 9 double2 chunks (chunk k = complex element k, row-major)
+//         addr = plane*9*Vh32 + (s>>5)*9*32 + k*32 + (s&31)
+//   FP32: 4 float4 chunks (complex elements 2k, 2k+1) in tiles, plus element 8
+//         as a plain float2 array:  addr4 = plane*4*Vh32 + (s>>5)*4*32 + k*32 + (s&31),
+//         addr2 = plane*Vh + s
+//   plane = mu*2 + parity.
 // The site index inside a parity plane is s = lex >> 1 with
 // lex = x + Nx(y + Ny(z + Nz t)), the reference's site order
 // (GLAC/parallelization/index.h:32-35); Nx must be even.
-// Traceless anti-Hermitian flow forces use 8 reals per link (a, d, b, c, e):
-//   FP64: 4 double2 chunks, FP32: 2 float4 chunks, same plane ordering.
+// Traceless anti-Hermitian flow forces use 8 reals per link (a, d, b, c, e) in
+// the same tiling: FP64 4 double2 chunks, FP32 2 float4 chunks.
 #pragma once
 
 #include <stdint.h>
@@ -118,51 +123,57 @@ GLAC_HD int parity_of_lex(const Geom &g, int lex) {
 // ---------------------------------------------------------------------------
 // Field accessors
 // ---------------------------------------------------------------------------
+GLAC_HD int round32(int v) { return (v + 31) & ~31; }
+
 template <typename T> struct LinkField;
 
 template <> struct LinkField<double> {
     double2 *p;
-    int Vh;
-    GLAC_HD size_t at(int mu, int par, int k, int s) const {
-        return ((size_t)((mu * 2 + par) * 9 + k)) * (size_t)Vh + (size_t)s;
+    int Vh, Vh32;
+    GLAC_HD size_t base(int mu, int par, int s) const {
+        return (size_t)(mu * 2 + par) * 9 * (size_t)Vh32 + (size_t)(s >> 5) * 288 + (size_t)(s & 31);
     }
     __device__ __forceinline__ M3<double> load(int mu, int par, int s) const {
+        const double2 *b = p + base(mu, par, s);
         M3<double> U;
 #pragma unroll
         for (int k = 0; k < 9; k++) {
-            double2 v = __ldg(p + at(mu, par, k, s));
+            double2 v = __ldg(b + 32 * k);
             U.e[k].re = v.x; U.e[k].im = v.y;
         }
         return U;
     }
     __device__ __forceinline__ M3<double> load_rw(int mu, int par, int s) const {
+        const double2 *b = p + base(mu, par, s);
         M3<double> U;
 #pragma unroll
         for (int k = 0; k < 9; k++) {
-            double2 v = p[at(mu, par, k, s)];
+            double2 v = b[32 * k];
             U.e[k].re = v.x; U.e[k].im = v.y;
         }
         return U;
     }
     __device__ __forceinline__ void store(int mu, int par, int s, const M3<double> &U) const {
+        double2 *b = p + base(mu, par, s);
 #pragma unroll
-        for (int k = 0; k < 9; k++) p[at(mu, par, k, s)] = make_double2(U.e[k].re, U.e[k].im);
+        for (int k = 0; k < 9; k++) b[32 * k] = make_double2(U.e[k].re, U.e[k].im);
     }
 };
 
 template <> struct LinkField<float> {
     float4 *p4;
     float2 *p2;
-    int Vh;
-    GLAC_HD size_t at4(int mu, int par, int k, int s) const {
-        return ((size_t)((mu * 2 + par) * 4 + k)) * (size_t)Vh + (size_t)s;
+    int Vh, Vh32;
+    GLAC_HD size_t base4(int mu, int par, int s) const {
+        return (size_t)(mu * 2 + par) * 4 * (size_t)Vh32 + (size_t)(s >> 5) * 128 + (size_t)(s & 31);
     }
     GLAC_HD size_t at2(int mu, int par, int s) const { return ((size_t)(mu * 2 + par)) * (size_t)Vh + (size_t)s; }
     __device__ __forceinline__ M3<float> load(int mu, int par, int s) const {
+        const float4 *b = p4 + base4(mu, par, s);
         M3<float> U;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            float4 v = __ldg(p4 + at4(mu, par, k, s));
+            float4 v = __ldg(b + 32 * k);
             U.e[2 * k].re = v.x; U.e[2 * k].im = v.y; U.e[2 * k + 1].re = v.z; U.e[2 * k + 1].im = v.w;
         }
         float2 w = __ldg(p2 + at2(mu, par, s));
@@ -170,10 +181,11 @@ template <> struct LinkField<float> {
         return U;
     }
     __device__ __forceinline__ M3<float> load_rw(int mu, int par, int s) const {
+        const float4 *b = p4 + base4(mu, par, s);
         M3<float> U;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            float4 v = p4[at4(mu, par, k, s)];
+            float4 v = b[32 * k];
             U.e[2 * k].re = v.x; U.e[2 * k].im = v.y; U.e[2 * k + 1].re = v.z; U.e[2 * k + 1].im = v.w;
         }
         float2 w = p2[at2(mu, par, s)];
@@ -181,9 +193,10 @@ template <> struct LinkField<float> {
         return U;
     }
     __device__ __forceinline__ void store(int mu, int par, int s, const M3<float> &U) const {
+        float4 *b = p4 + base4(mu, par, s);
 #pragma unroll
         for (int k = 0; k < 4; k++)
-            p4[at4(mu, par, k, s)] = make_float4(U.e[2 * k].re, U.e[2 * k].im, U.e[2 * k + 1].re, U.e[2 * k + 1].im);
+            b[32 * k] = make_float4(U.e[2 * k].re, U.e[2 * k].im, U.e[2 * k + 1].re, U.e[2 * k + 1].im);
         p2[at2(mu, par, s)] = make_float2(U.e[8].re, U.e[8].im);
     }
 };
@@ -192,42 +205,45 @@ template <typename T> struct ForceField;
 
 template <> struct ForceField<double> {
     double2 *p;
-    int Vh;
-    GLAC_HD size_t at(int mu, int par, int k, int s) const {
-        return ((size_t)((mu * 2 + par) * 4 + k)) * (size_t)Vh + (size_t)s;
+    int Vh, Vh32;
+    GLAC_HD size_t base(int mu, int par, int s) const {
+        return (size_t)(mu * 2 + par) * 4 * (size_t)Vh32 + (size_t)(s >> 5) * 128 + (size_t)(s & 31);
     }
     __device__ __forceinline__ AH8<double> load(int mu, int par, int s) const {
+        const double2 *b = p + base(mu, par, s);
         AH8<double> Z;
-        double2 v0 = p[at(mu, par, 0, s)], v1 = p[at(mu, par, 1, s)], v2 = p[at(mu, par, 2, s)],
-                v3 = p[at(mu, par, 3, s)];
+        double2 v0 = b[0], v1 = b[32], v2 = b[64], v3 = b[96];
         Z.a = v0.x; Z.d = v0.y;
         Z.b = cx(v1.x, v1.y); Z.c = cx(v2.x, v2.y); Z.e = cx(v3.x, v3.y);
         return Z;
     }
     __device__ __forceinline__ void store(int mu, int par, int s, const AH8<double> &Z) const {
-        p[at(mu, par, 0, s)] = make_double2(Z.a, Z.d);
-        p[at(mu, par, 1, s)] = make_double2(Z.b.re, Z.b.im);
-        p[at(mu, par, 2, s)] = make_double2(Z.c.re, Z.c.im);
-        p[at(mu, par, 3, s)] = make_double2(Z.e.re, Z.e.im);
+        double2 *b = p + base(mu, par, s);
+        b[0] = make_double2(Z.a, Z.d);
+        b[32] = make_double2(Z.b.re, Z.b.im);
+        b[64] = make_double2(Z.c.re, Z.c.im);
+        b[96] = make_double2(Z.e.re, Z.e.im);
     }
 };
 
 template <> struct ForceField<float> {
     float4 *p;
-    int Vh;
-    GLAC_HD size_t at(int mu, int par, int k, int s) const {
-        return ((size_t)((mu * 2 + par) * 2 + k)) * (size_t)Vh + (size_t)s;
+    int Vh, Vh32;
+    GLAC_HD size_t base(int mu, int par, int s) const {
+        return (size_t)(mu * 2 + par) * 2 * (size_t)Vh32 + (size_t)(s >> 5) * 64 + (size_t)(s & 31);
     }
     __device__ __forceinline__ AH8<float> load(int mu, int par, int s) const {
+        const float4 *b = p + base(mu, par, s);
         AH8<float> Z;
-        float4 v0 = p[at(mu, par, 0, s)], v1 = p[at(mu, par, 1, s)];
+        float4 v0 = b[0], v1 = b[32];
         Z.a = v0.x; Z.d = v0.y; Z.b = cx(v0.z, v0.w);
         Z.c = cx(v1.x, v1.y); Z.e = cx(v1.z, v1.w);
         return Z;
     }
     __device__ __forceinline__ void store(int mu, int par, int s, const AH8<float> &Z) const {
-        p[at(mu, par, 0, s)] = make_float4(Z.a, Z.d, Z.b.re, Z.b.im);
-        p[at(mu, par, 1, s)] = make_float4(Z.c.re, Z.c.im, Z.e.re, Z.e.im);
+        float4 *b = p + base(mu, par, s);
+        b[0] = make_float4(Z.a, Z.d, Z.b.re, Z.b.im);
+        b[32] = make_float4(Z.c.re, Z.c.im, Z.e.re, Z.e.im);
     }
 };
 

@@ -489,31 +489,37 @@ void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
-/* uniform in (-1/2, 1/2), never 0 */
-static double u_sym(uint32_t w) { return ((double)w + 0.5) * 2.3283064365386963e-10 - 0.5; }
+/* uniform in (-1/2, 1/2) from 16 bits, never 0 */
+static double u_sym16(uint32_t h) { return ((double)h + 0.5) * (1.0 / 65536.0) - 0.5; }
 /* uniform in [0, 1) with 53 bits */
 static double u_53(uint32_t hi, uint32_t lo) {
     return (double)(((uint64_t)hi << 21) | (lo >> 11)) * 1.1102230246251565e-16;
 }
 
-/* Proposal for (link id, hit) from the Philox stream: 12 uniforms build R, S, T
- * (su3matrixgenerator.h:170-196), bit 31 of the 13th word chooses X or X^+,
- * words 14-15 give the accept uniform. */
+/* Proposal for (link id, hit) from the Philox stream: two calls give 8 words;
+ * words 0-5 hold twelve 16-bit uniforms (low half first) that build R, S, T
+ * (su3matrixgenerator.h:170-196), words 6-7 the 53-bit accept uniform, and bit
+ * 0 of word 7 chooses X or X^+. */
 static void proposal(uint32_t key[2], uint32_t link_id, uint32_t sweep, uint32_t stream, int hit,
                      double eps, double *X, double *r) {
-    uint32_t w[16];
-    for (int call = 0; call < 4; call++) {
-        uint32_t ctr[4] = {(uint32_t)(4 * hit + call), link_id, sweep, stream};
+    uint32_t w[8];
+    for (int call = 0; call < 2; call++) {
+        uint32_t ctr[4] = {(uint32_t)(2 * hit + call), link_id, sweep, stream};
         oracle_philox4x32_10(ctr, key, w + 4 * call);
     }
     double su2[3][8];
     for (int b = 0; b < 3; b++) {
-        double u[4] = {u_sym(w[4 * b]), u_sym(w[4 * b + 1]), u_sym(w[4 * b + 2]), u_sym(w[4 * b + 3])};
+        double u[4];
+        for (int c = 0; c < 4; c++) {
+            int k = 4 * b + c;
+            uint32_t word = w[k >> 1];
+            u[c] = u_sym16((k & 1) ? (word >> 16) : (word & 0xFFFFu));
+        }
         oracle_su2_near_unity(u, eps, su2[b]);
     }
-    int inverse = (w[12] & 0x80000000u) == 0u;
+    int inverse = (w[7] & 1u) == 0u;
     oracle_rst_multiply(su2[0], su2[1], su2[2], inverse, X);
-    *r = u_53(w[13], w[14]);
+    *r = u_53(w[6], w[7]);
 }
 
 uint64_t oracle_metropolis_sweep(const int N[4], double *links, double beta, double eps,

@@ -71,7 +71,7 @@ void oracle_accept_fed(long nlinks, int nhits, double beta, double *U, const dou
 /* Checkerboard Metropolis with Philox streams (project design, no reference
  * counterpart): sub-sweep k = 2*mu + parity; for each link of that class the
  * staple is taken once and nhits proposals drawn from the Philox stream
- * (key = seed, counter = {4*hit + call, mu*V + site, sweep, stream}).
+ * (key = seed, counter = {2*hit + call, mu*V + site, sweep, stream}).
  * Returns accepted proposals; links updated in place. */
 uint64_t oracle_metropolis_sweep(const int N[4], double *links, double beta, double eps,
                                  int nhits, uint64_t seed, uint32_t stream, uint32_t sweep);
