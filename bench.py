@@ -258,7 +258,7 @@ def run_gpu(args):
     achieved = alg_bytes / stage_total_s / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(achieved / hbm_peak, 4), "traffic": None,
-                "kernel": "k_flow_stage_pair (3 RK3 stages per step)",
+                "kernel": "k_flow_stage<f32x2> (3 RK3 stages per step)",
                 "bytes_per_site_step": sum(STAGE_BYTES_FP32), "peak_source": peak_kind,
                 "stage_ms": [round(x * 1e3, 4) for x in st]}
 
@@ -359,8 +359,6 @@ def run_profile(args):
     import glac_b200 as g
     dims = tuple(int(x) for x in args.dims.split(","))
     L = g.Lattice(dims, beta=BETA, precision=args.precision, flow_eps=FLOW_EPS, seed=5, device=0)
-    if args.variant:
-        L.set_option("pair_kernel", 1 if args.variant == "pair" else 0)
     L.hot_start(7)
     if args.profile == "metropolis":
         L.metropolis(args.steps)
@@ -381,7 +379,7 @@ def run_profile(args):
         sec = e0.elapsed_time(e1) / 1e3 / args.time_reps
         stages = L.flow_stage_times(5) if args.profile == "flow" else None
         print(json.dumps({"profile": args.profile, "dims": dims, "precision": args.precision,
-                          "variant": args.variant, "ms_per_step": sec * 1e3,
+                          "ms_per_step": sec * 1e3,
                           "rate": (4 * V if args.profile == "metropolis" else V) / sec,
                           "stage_ms": None if stages is None else [x * 1e3 for x in stages]}))
     L.close()
@@ -398,7 +396,6 @@ def main():
     ap.add_argument("--profile", choices=["flow", "metropolis"], help="small workload for ncu / variant timing")
     ap.add_argument("--dims", default="32,32,32,64")
     ap.add_argument("--precision", default="fp32")
-    ap.add_argument("--variant", default="", choices=["", "pair", "scalar"])
     ap.add_argument("--no-obs", action="store_true")
     ap.add_argument("--time-reps", type=int, default=0)
     args = ap.parse_args()

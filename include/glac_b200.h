@@ -44,7 +44,7 @@ typedef enum { GLAC_FP64 = 0, GLAC_FP32 = 1 } glac_precision;
 typedef enum { GLAC_EXP_MORNINGSTAR = 0, GLAC_EXP_LUSCHER = 1, GLAC_EXP_TAYLOR2 = 2, GLAC_EXP_TAYLOR4 = 3 } glac_exp;
 
 typedef struct {
-    int dims[4];            /* Nx, Ny, Nz, Nt; each even and >= 4 (NSpatial/NTemporal) */
+    int dims[4];            /* Nx, Ny, Nz, Nt; each even and >= 4, Nt % 4 == 0 for FP32 (NSpatial/NTemporal) */
     double beta;            /* "beta" */
     int precision;          /* glac_precision */
     int n_updates;          /* "NUpdates": Metropolis hits per link */
@@ -71,7 +71,7 @@ void *glac_stream(glac_ctx *ctx);
 glac_status glac_sync(glac_ctx *ctx);
 /* Number of kernels this context has launched so far. */
 uint64_t glac_launch_count(const glac_ctx *ctx);
-/* Tuning switches: "pair_kernel" (FP32 flow in packed f32x2 lanes, default 1). */
+/* Tuning switches by name (none defined at present; unknown keys give GLAC_ERR_ARG). */
 glac_status glac_set_option(glac_ctx *ctx, const char *key, long value);
 
 /* ---- field --------------------------------------------------------------- */

@@ -109,16 +109,30 @@ def test_flow_and_observables_vs_reference(g, golden, prec):
         assert rel_err(L.get_links(), golden["flow3"]) < TOL[prec]
 
 
-def test_fp32_scalar_and_packed_flow_agree(g, golden):
-    outs = []
-    for pair in (0, 1):
-        with lattice(g, N4, "fp32", flow_eps=0.01) as L:
-            L.set_option("pair_kernel", pair)
-            L.set_links(golden["links"])
-            L.flow(3, measure=False)
-            outs.append(L.get_links())
-    assert rel_err(outs[0], golden["flow3"]) < 1e-5
-    assert rel_err(outs[1], outs[0]) < 1e-5
+def test_fp32_lanes_across_the_t_cut(g, oracle):
+    # FP32 carries t and t + Nt/2 in the two lanes of one thread; a field that
+    # differs strongly between the halves checks the lane swap at the cut
+    N = (4, 4, 4, 8)
+    links = oracle.haar_field(N, 314)
+    V = int(np.prod(N))
+    half = V // 2
+    cold = np.zeros((4, half, 18))
+    cold[:, :, [0, 8, 16]] = 1.0
+    links[:, half:] = cold  # upper half in t is cold
+    want_obs = oracle.observables(N, links)
+    want_flow = oracle.flow(N, links, 0.02, 2)
+    with lattice(g, N, "fp32", flow_eps=0.02) as L:
+        L.set_links(links)
+        assert rel_err(L.measure(), want_obs) < 1e-5
+        assert rel_err(L.staples(), oracle.staples(N, links)) < 1e-5
+        L.flow(2, measure=False)
+        assert rel_err(L.get_links(), want_flow) < 1e-5
+
+
+def test_fp32_needs_nt_multiple_of_four(g):
+    with pytest.raises(g.GlacError) as e:
+        g.Lattice((4, 4, 4, 6), precision="fp32")
+    assert e.value.status == g.GLAC_ERR_ARG
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
