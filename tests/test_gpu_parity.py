@@ -116,9 +116,13 @@ def test_fp32_lanes_across_the_t_cut(g, oracle):
     links = oracle.haar_field(N, 314)
     V = int(np.prod(N))
     half = V // 2
-    cold = np.zeros((4, half, 18))
-    cold[:, :, [0, 8, 16]] = 1.0
-    links[:, half:] = cold  # upper half in t is cold
+    rng = np.random.default_rng(7)
+    H = rng.standard_normal((4 * half, 3, 3)) + 1j * rng.standard_normal((4 * half, 3, 3))
+    Z = 0.05 * (H - np.conj(np.transpose(H, (0, 2, 1))))
+    Z -= np.eye(3) * (np.trace(Z, axis1=1, axis2=2)[:, None, None] / 3)
+    m = np.empty((4 * half, 18))
+    m[:, 0::2], m[:, 1::2] = Z.real.reshape(-1, 9), Z.imag.reshape(-1, 9)
+    links[:, half:] = oracle.exp(m, 0).reshape(4, half, 18)  # upper half in t: near unity
     want_obs = oracle.observables(N, links)
     want_flow = oracle.flow(N, links, 0.02, 2)
     with lattice(g, N, "fp32", flow_eps=0.02) as L:
