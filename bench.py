@@ -224,6 +224,7 @@ def run_gpu(args):
     L.hot_start(20261203)
     L.metropolis(5)
     L.reunitarize()
+    tuned = L.autotune(3)
     acc_holder = {}
     t_metro = timed(lambda: acc_holder.setdefault("a", L.metropolis(1)), 20)
     L.metropolis(THERM_SWEEPS - 25)
@@ -310,6 +311,7 @@ def run_gpu(args):
             "metropolis_link_updates_per_s_fp32": metro_rate,
             "metropolis_acceptance": acc_holder.get("a"),
             "plaq_after_flow": float(obs_last[0]),
+            "autotune": tuned,
         },
     }
     if cpu_base:
@@ -360,6 +362,8 @@ def run_profile(args):
     dims = tuple(int(x) for x in args.dims.split(","))
     L = g.Lattice(dims, beta=BETA, precision=args.precision, flow_eps=FLOW_EPS, seed=5, device=0)
     L.hot_start(7)
+    if args.tune:
+        L.tuning = [int(x) for x in args.tune.split(",")]
     if args.profile == "metropolis":
         L.metropolis(args.steps)
     else:
@@ -378,7 +382,7 @@ def run_profile(args):
         torch.cuda.synchronize()
         sec = e0.elapsed_time(e1) / 1e3 / args.time_reps
         stages = L.flow_stage_times(5) if args.profile == "flow" else None
-        print(json.dumps({"profile": args.profile, "dims": dims, "precision": args.precision,
+        print(json.dumps({"profile": args.profile, "dims": dims, "precision": args.precision, "tune": L.tuning,
                           "ms_per_step": sec * 1e3,
                           "rate": (4 * V if args.profile == "metropolis" else V) / sec,
                           "stage_ms": None if stages is None else [x * 1e3 for x in stages]}))
@@ -398,6 +402,7 @@ def main():
     ap.add_argument("--precision", default="fp32")
     ap.add_argument("--no-obs", action="store_true")
     ap.add_argument("--time-reps", type=int, default=0)
+    ap.add_argument("--tune", default="", help="launch variants flow,metropolis,observables (profile mode)")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)

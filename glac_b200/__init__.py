@@ -99,6 +99,9 @@ def lib() -> C.CDLL:
     L.glac_measure.argtypes = [P, C.c_void_p]
     L.glac_flow_configuration.argtypes = [P, C.c_void_p, C.c_int, C.c_void_p]
     L.glac_flow_stage_times.argtypes = [P, C.c_int, _dp]
+    L.glac_autotune.argtypes = [P, C.c_int, C.c_void_p]
+    L.glac_get_tuning.argtypes = [P, C.c_void_p]
+    L.glac_set_tuning.argtypes = [P, C.c_void_p]
     L.glac_staples.argtypes = [P, _dp]
     L.glac_force.argtypes = [P, _dp]
     L.glac_exp_batch.argtypes = [C.c_int, C.c_int, _dp, C.c_long, _dp]
@@ -239,6 +242,26 @@ class Lattice:
             out = np.empty((n_steps + 1, 3 + self.Nt), np.float64)
         self._ck(lib().glac_flow(self._ctx, int(n_steps), out.ctypes.data))
         return out
+
+    def autotune(self, reps: int = 3):
+        """Pick the fastest launch variant of each kernel family on this lattice;
+        returns the timing table {family: [seconds per call per variant]}."""
+        rep = np.zeros(12)
+        self._ck(lib().glac_autotune(self._ctx, int(reps), rep.ctypes.data))
+        rep = rep.reshape(3, 4)
+        return {"flow": rep[0].tolist(), "metropolis": rep[1].tolist(), "observables": rep[2].tolist(),
+                "chosen": self.tuning}
+
+    @property
+    def tuning(self):
+        v = np.zeros(3, np.int32)
+        self._ck(lib().glac_get_tuning(self._ctx, v.ctypes.data))
+        return v.tolist()
+
+    @tuning.setter
+    def tuning(self, variants):
+        v = np.ascontiguousarray(variants, np.int32)
+        self._ck(lib().glac_set_tuning(self._ctx, v.ctypes.data))
 
     def flow_stage_times(self, n_steps: int):
         out = np.zeros(3)

@@ -29,6 +29,7 @@ struct glac_ctx {
     double *scalar_dev = nullptr;
     uint32_t sweep = 0;
     uint64_t launches = 0;
+    int tune[3] = {0, 0, 0};  // chosen launch variant per kernel family (flow, metropolis, observables)
     bool has_field = false;
     std::string err;
 };
@@ -48,11 +49,16 @@ void ck(cudaError_t e, const char *what) {
 }
 void ck_launch(const char *what) { ck(cudaGetLastError(), what); }
 
-// 8 planes of Vh32 tiled stored sites (see lattice.cuh): 9 x 16-byte chunks per
-// link (FP64 one site, FP32 two sites in lanes), 4 chunks per force.
-size_t field_bytes(const glac_desc &, const Geom &g) { return 8 * (size_t)round32(g.Vh) * 9 * 16; }
-size_t force_bytes(const glac_desc &, const Geom &g) { return 8 * (size_t)round32(g.Vh) * 4 * 16; }
-size_t host_field_doubles(const Geom &g) { return (size_t)g.V * g.lanes * 72; }
+// 8 planes of Vh32 tiled sites (see lattice.cuh); FP32 adds the plain float2 plane array.
+size_t field_bytes(const glac_desc &d, const Geom &g) {
+    const size_t vh32 = (size_t)round32(g.Vh);
+    if (d.precision == GLAC_FP64) return 8 * vh32 * 9 * sizeof(double2);
+    return 8 * vh32 * 4 * sizeof(float4) + 8 * (size_t)g.Vh * sizeof(float2);
+}
+size_t force_bytes(const glac_desc &d, const Geom &g) {
+    const size_t vh32 = (size_t)round32(g.Vh);
+    return d.precision == GLAC_FP64 ? 8 * vh32 * 4 * sizeof(double2) : 8 * vh32 * 2 * sizeof(float4);
+}
 
 LinkField<double> f64(glac_ctx *c, int i) {
     LinkField<double> L;
@@ -61,11 +67,12 @@ LinkField<double> f64(glac_ctx *c, int i) {
     L.Vh32 = round32(c->g.Vh);
     return L;
 }
-LinkField<f32x2> f32(glac_ctx *c, int i) {
-    LinkField<f32x2> L;
-    L.p = reinterpret_cast<float4 *>(c->field[i]);
+LinkField<float> f32(glac_ctx *c, int i) {
+    LinkField<float> L;
     L.Vh = c->g.Vh;
     L.Vh32 = round32(c->g.Vh);
+    L.p4 = reinterpret_cast<float4 *>(c->field[i]);
+    L.p2 = reinterpret_cast<float2 *>(L.p4 + (size_t)8 * 4 * L.Vh32);
     return L;
 }
 ForceField<double> z64(glac_ctx *c) {
@@ -75,8 +82,8 @@ ForceField<double> z64(glac_ctx *c) {
     Z.Vh32 = round32(c->g.Vh);
     return Z;
 }
-ForceField<f32x2> z32(glac_ctx *c) {
-    ForceField<f32x2> Z;
+ForceField<float> z32(glac_ctx *c) {
+    ForceField<float> Z;
     Z.p = reinterpret_cast<float4 *>(c->force);
     Z.Vh = c->g.Vh;
     Z.Vh32 = round32(c->g.Vh);
@@ -100,7 +107,7 @@ glac_status guarded(glac_ctx *c, F &&f) {
 }
 
 void ensure_staging(glac_ctx *c) {
-    if (!c->staging) ck(cudaMalloc(&c->staging, host_field_doubles(c->g) * sizeof(double)), "cudaMalloc staging");
+    if (!c->staging) ck(cudaMalloc(&c->staging, (size_t)c->g.V * 4 * 18 * sizeof(double)), "cudaMalloc staging");
 }
 void ensure_obs(glac_ctx *c, size_t n) {
     if (c->obs_cap >= n) return;
@@ -111,8 +118,10 @@ void ensure_obs(glac_ctx *c, size_t n) {
 }
 
 void measure_into(glac_ctx *c, double *dev_out) {
-    if (c->d.precision == GLAC_FP64) launch_observables(c->g, f64(c, c->cur), c->plan, c->partial, dev_out, c->stream);
-    else launch_observables(c->g, f32(c, c->cur), c->plan, c->partial, dev_out, c->stream);
+    if (c->d.precision == GLAC_FP64)
+        launch_observables(c->g, f64(c, c->cur), c->plan, c->partial, dev_out, c->tune[FAM_OBS], c->stream);
+    else
+        launch_observables(c->g, f32(c, c->cur), c->plan, c->partial, dev_out, c->tune[FAM_OBS], c->stream);
     ck_launch("observables");
     c->launches += 2;
 }
@@ -135,10 +144,10 @@ void flow_step(glac_ctx *c, cudaEvent_t *ev = nullptr) {
         const int src = c->cur, dst = c->cur ^ 1;
         if (c->d.precision == GLAC_FP64)
             launch_flow_stage(c->g, f64(c, src), f64(c, dst), z64(c), stage, c->d.exp_func, alpha[stage],
-                              beta[stage], c->stream);
+                              beta[stage], c->tune[FAM_FLOW], c->stream);
         else
             launch_flow_stage(c->g, f32(c, src), f32(c, dst), z32(c), stage, c->d.exp_func, alpha[stage],
-                              beta[stage], c->stream);
+                              beta[stage], c->tune[FAM_FLOW], c->stream);
         ck_launch("flow stage");
         c->launches += 1;
         c->cur = dst;
@@ -181,20 +190,16 @@ glac_status glac_create(const glac_desc *desc, glac_ctx **out) {
     if (d.n_updates < 0) { g_global_err = "n_updates must be >= 0"; return GLAC_ERR_ARG; }
     if (!(d.su3_eps > 0.0 && d.su3_eps < 1.0)) { g_global_err = "su3_eps must lie in (0, 1)"; return GLAC_ERR_ARG; }
     if (d.dims[3] > 1024) { g_global_err = "Nt > 1024 is not supported"; return GLAC_ERR_ARG; }
-    if (d.precision == GLAC_FP32 && d.dims[3] % 4) {
-        g_global_err = "FP32 needs Nt divisible by 4 (the two t halves share a thread)";
-        return GLAC_ERR_ARG;
-    }
     glac_ctx *c = new glac_ctx();
     c->d = d;
-    c->g = make_geom(d.dims, d.precision == GLAC_FP32 ? 2 : 1);
+    c->g = make_geom(d.dims);
     c->plan = make_obs_plan(c->g);
     try {
         ck(cudaSetDevice(d.device), "cudaSetDevice");
         ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         for (int i = 0; i < 2; i++) ck(cudaMalloc(&c->field[i], field_bytes(d, c->g)), "cudaMalloc field");
         ck(cudaMalloc(&c->force, force_bytes(d, c->g)), "cudaMalloc force");
-        ck(cudaMalloc(&c->partial, (size_t)kObsPartial * c->plan.nblocks * sizeof(double)), "cudaMalloc partials");
+        ck(cudaMalloc(&c->partial, (size_t)3 * c->plan.nblocks * sizeof(double)), "cudaMalloc partials");
         ck(cudaMalloc(&c->acc_dev, sizeof(unsigned long long)), "cudaMalloc counter");
         ck(cudaMalloc(&c->scalar_dev, sizeof(double)), "cudaMalloc scalar");
         ensure_obs(c, 3 + (size_t)d.dims[3]);
@@ -286,7 +291,7 @@ glac_status glac_set_links(glac_ctx *c, const double *host) {
     return guarded(c, [&] {
         if (!host) { c->err = "null field"; return GLAC_ERR_ARG; }
         ensure_staging(c);
-        ck(cudaMemcpyAsync(c->staging, host, host_field_doubles(c->g) * sizeof(double), cudaMemcpyHostToDevice,
+        ck(cudaMemcpyAsync(c->staging, host, (size_t)c->g.V * 72 * sizeof(double), cudaMemcpyHostToDevice,
                            c->stream),
            "H2D links");
         glac_status s = glac_set_links_device(c, c->staging);
@@ -302,7 +307,7 @@ glac_status glac_get_links(glac_ctx *c, double *host) {
         ensure_staging(c);
         glac_status s = glac_get_links_device(c, c->staging);
         if (s != GLAC_OK) return s;
-        ck(cudaMemcpyAsync(host, c->staging, host_field_doubles(c->g) * sizeof(double), cudaMemcpyDeviceToHost,
+        ck(cudaMemcpyAsync(host, c->staging, (size_t)c->g.V * 72 * sizeof(double), cudaMemcpyDeviceToHost,
                            c->stream),
            "D2H links");
         ck(cudaStreamSynchronize(c->stream), "sync");
@@ -344,10 +349,12 @@ glac_status glac_metropolis(glac_ctx *c, int n_sweeps, double *acceptance) {
                 const int mu = k >> 1, p = k & 1;
                 if (c->d.precision == GLAC_FP64)
                     launch_metropolis(c->g, f64(c, c->cur), mu, p, c->d.beta, c->d.su3_eps, c->d.n_updates,
-                                      c->d.seed, c->sweep, c->d.stream_id, c->acc_dev, c->stream);
+                                      c->d.seed, c->sweep, c->d.stream_id, c->acc_dev, c->tune[FAM_METRO],
+                                      c->stream);
                 else
                     launch_metropolis(c->g, f32(c, c->cur), mu, p, c->d.beta, c->d.su3_eps, c->d.n_updates,
-                                      c->d.seed, c->sweep, c->d.stream_id, c->acc_dev, c->stream);
+                                      c->d.seed, c->sweep, c->d.stream_id, c->acc_dev, c->tune[FAM_METRO],
+                                      c->stream);
                 ck_launch("metropolis");
                 c->launches++;
             }
@@ -359,8 +366,7 @@ glac_status glac_metropolis(glac_ctx *c, int n_sweeps, double *acceptance) {
             unsigned long long acc = 0;
             ck(cudaMemcpyAsync(&acc, c->acc_dev, sizeof(acc), cudaMemcpyDeviceToHost, c->stream), "D2H");
             ck(cudaStreamSynchronize(c->stream), "sync");
-            const double per = 4.0 * (double)c->d.n_updates * (double)c->g.V * c->g.lanes *
-                               (double)(n_sweeps > 0 ? n_sweeps : 1);
+            const double per = 4.0 * (double)c->d.n_updates * (double)c->g.V * (double)(n_sweeps > 0 ? n_sweeps : 1);
             *acceptance = per > 0 ? (double)acc / per : 0.0;
         }
         return GLAC_OK;
@@ -371,7 +377,7 @@ glac_status glac_measure(glac_ctx *c, double *obs) {
     return guarded(c, [&] {
         glac_status s = need_field(c);
         if (s != GLAC_OK) return s;
-        const size_t n = 3 + (size_t)c->d.dims[3];
+        const size_t n = 3 + (size_t)c->g.N[3];
         ensure_obs(c, n);
         measure_into(c, c->obs_dev);
         if (obs) {
@@ -387,7 +393,7 @@ glac_status glac_flow(glac_ctx *c, int n_steps, double *obs) {
         glac_status s = need_field(c);
         if (s != GLAC_OK) return s;
         if (n_steps < 0) { c->err = "n_steps < 0"; return GLAC_ERR_ARG; }
-        const size_t per = 3 + (size_t)c->d.dims[3];
+        const size_t per = 3 + (size_t)c->g.N[3];
         if (obs) {
             ensure_obs(c, per * (size_t)(n_steps + 1));
             measure_into(c, c->obs_dev);
@@ -431,6 +437,99 @@ glac_status glac_flow_stage_times(glac_ctx *c, int n_steps, double *seconds3) {
     });
 }
 
+// Launch-variant autotuner: times every variant of the flow-stage, Metropolis
+// and observable kernels on this context's lattice and keeps the fastest.
+// The field, the sweep counter and the Philox stream are restored afterwards.
+// report (optional, 3 x kMaxVariants doubles) receives the mean seconds per
+// call of each variant (0 where a family has fewer variants).
+glac_status glac_autotune(glac_ctx *c, int reps, double *report) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        if (reps <= 0) reps = 3;
+        const bool fp32 = c->d.precision == GLAC_FP32;
+        void *backup = nullptr;
+        ck(cudaMalloc(&backup, field_bytes(c->d, c->g)), "cudaMalloc autotune backup");
+        ck(cudaMemcpyAsync(backup, c->field[c->cur], field_bytes(c->d, c->g), cudaMemcpyDeviceToDevice, c->stream),
+           "backup");
+        const uint32_t sweep0 = c->sweep;
+        const int cur0 = c->cur;
+        cudaEvent_t e0, e1;
+        ck(cudaEventCreate(&e0), "event");
+        ck(cudaEventCreate(&e1), "event");
+        auto restore = [&]() {
+            c->cur = cur0;
+            c->sweep = sweep0;
+            ck(cudaMemcpyAsync(c->field[c->cur], backup, field_bytes(c->d, c->g), cudaMemcpyDeviceToDevice,
+                               c->stream),
+               "restore");
+        };
+        double table[3][kMaxVariants] = {{0}};
+        for (int fam = 0; fam < 3; fam++) {
+            const int nv = num_variants((Family)fam, fp32);
+            int best = 0;
+            double best_t = 1e300;
+            for (int v = 0; v < nv; v++) {
+                c->tune[fam] = v;
+                for (int pass = 0; pass < 2; pass++) {  // pass 0 warms up
+                    ck(cudaEventRecord(e0, c->stream), "event");
+                    for (int r = 0; r < reps; r++) {
+                        if (fam == FAM_FLOW) flow_step(c);
+                        else if (fam == FAM_METRO) {
+                            for (int k = 0; k < 8; k++) {
+                                if (fp32)
+                                    launch_metropolis(c->g, f32(c, c->cur), k >> 1, k & 1, c->d.beta, c->d.su3_eps,
+                                                      c->d.n_updates, c->d.seed, c->sweep, c->d.stream_id, c->acc_dev,
+                                                      v, c->stream);
+                                else
+                                    launch_metropolis(c->g, f64(c, c->cur), k >> 1, k & 1, c->d.beta, c->d.su3_eps,
+                                                      c->d.n_updates, c->d.seed, c->sweep, c->d.stream_id, c->acc_dev,
+                                                      v, c->stream);
+                                ck_launch("metropolis");
+                            }
+                        } else measure_into(c, c->obs_dev);
+                    }
+                    ck(cudaEventRecord(e1, c->stream), "event");
+                    ck(cudaEventSynchronize(e1), "event sync");
+                    restore();
+                }
+                float ms = 0.f;
+                ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+                const double t = ms * 1e-3 / reps;
+                table[fam][v] = t;
+                if (t < best_t) { best_t = t; best = v; }
+            }
+            c->tune[fam] = best;
+        }
+        ck(cudaStreamSynchronize(c->stream), "sync");
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaFree(backup);
+        if (report)
+            for (int f = 0; f < 3; f++)
+                for (int v = 0; v < kMaxVariants; v++) report[3 * 0 + f * kMaxVariants + v] = table[f][v];
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_get_tuning(glac_ctx *c, int *variants3) {
+    if (!c || !variants3) return GLAC_ERR_ARG;
+    for (int f = 0; f < 3; f++) variants3[f] = c->tune[f];
+    return GLAC_OK;
+}
+
+glac_status glac_set_tuning(glac_ctx *c, const int *variants3) {
+    if (!c || !variants3) return GLAC_ERR_ARG;
+    const bool fp32 = c->d.precision == GLAC_FP32;
+    for (int f = 0; f < 3; f++)
+        if (variants3[f] < 0 || variants3[f] >= num_variants((Family)f, fp32)) {
+            c->err = "tuning variant out of range";
+            return GLAC_ERR_ARG;
+        }
+    for (int f = 0; f < 3; f++) c->tune[f] = variants3[f];
+    return GLAC_OK;
+}
+
 glac_status glac_flow_configuration(glac_ctx *c, const double *host_links, int n_steps, double *obs) {
     glac_status s = glac_set_links(c, host_links);
     if (s != GLAC_OK) return s;
@@ -442,11 +541,11 @@ glac_status glac_staples(glac_ctx *c, double *host_out) {
         glac_status s = need_field(c);
         if (s != GLAC_OK) return s;
         ensure_staging(c);
-        if (c->d.precision == GLAC_FP64) launch_staples_aos(c->g, f64(c, c->cur), c->staging, 0, c->stream);
-        else launch_staples_aos(c->g, f32(c, c->cur), c->staging, 0, c->stream);
+        if (c->d.precision == GLAC_FP64) launch_staples_aos(c->g, f64(c, c->cur), c->staging, c->stream);
+        else launch_staples_aos(c->g, f32(c, c->cur), c->staging, c->stream);
         ck_launch("staples");
         c->launches++;
-        ck(cudaMemcpyAsync(host_out, c->staging, host_field_doubles(c->g) * sizeof(double), cudaMemcpyDeviceToHost,
+        ck(cudaMemcpyAsync(host_out, c->staging, (size_t)c->g.V * 72 * sizeof(double), cudaMemcpyDeviceToHost,
                            c->stream),
            "D2H");
         ck(cudaStreamSynchronize(c->stream), "sync");
@@ -459,11 +558,11 @@ glac_status glac_force(glac_ctx *c, double *host_out) {
         glac_status s = need_field(c);
         if (s != GLAC_OK) return s;
         ensure_staging(c);
-        if (c->d.precision == GLAC_FP64) launch_staples_aos(c->g, f64(c, c->cur), c->staging, 1, c->stream);
-        else launch_staples_aos(c->g, f32(c, c->cur), c->staging, 1, c->stream);
+        if (c->d.precision == GLAC_FP64) launch_force_aos(c->g, f64(c, c->cur), c->staging, c->stream);
+        else launch_force_aos(c->g, f32(c, c->cur), c->staging, c->stream);
         ck_launch("force");
         c->launches++;
-        ck(cudaMemcpyAsync(host_out, c->staging, host_field_doubles(c->g) * sizeof(double), cudaMemcpyDeviceToHost,
+        ck(cudaMemcpyAsync(host_out, c->staging, (size_t)c->g.V * 72 * sizeof(double), cudaMemcpyDeviceToHost,
                            c->stream),
            "D2H");
         ck(cudaStreamSynchronize(c->stream), "sync");

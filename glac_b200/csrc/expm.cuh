@@ -124,20 +124,6 @@ template <typename R> GLAC_HD void invariants(const HQ<R> &Q, const HQ2<R> &S, R
     o = fmaR(Q.z.im, S.z.im, o);
     c0 = (t + o + o) * R(0.33333333333333333);
 }
-template <> GLAC_HD void invariants<f32x2>(const HQ<f32x2> &Q, const HQ2<f32x2> &S, f32x2 &c0, f32x2 &c1) {
-    c1 = f32x2(0.5f) * (S.d0 + S.d1 + S.d2);
-    f32x2 t = Q.q0 * S.d0;
-    t = fmaR(Q.q1, S.d1, t);
-    t = fmaR(Q.q2, S.d2, t);
-    f32x2 o = Q.x.re * S.x.re;
-    o = fmaR(Q.x.im, S.x.im, o);
-    o = fmaR(Q.y.re, S.y.re, o);
-    o = fmaR(Q.y.im, S.y.im, o);
-    o = fmaR(Q.z.re, S.z.re, o);
-    o = fmaR(Q.z.im, S.z.im, o);
-    c0 = (t + o + o) * f32x2(0.33333334f);
-}
-
 template <typename R> struct SeriesTerms { static const int n = 9; };
 template <> struct SeriesTerms<double> { static const int n = 16; };
 #define GLAC_SERIES_C1_MAX 0.1
@@ -219,26 +205,6 @@ template <typename R> GLAC_HD M3<R> expm_morningstar(const AH8<R> &Z) {
         f0 = cx(from_d<R>(f.f0r), from_d<R>(f.f0i));
         f1 = cx(from_d<R>(f.f1r), from_d<R>(f.f1i));
         f2 = cx(from_d<R>(f.f2r), from_d<R>(f.f2i));
-    }
-    return ms_combine(Q, S, f0, f1, f2);
-}
-
-// Packed pair: the series in packed FP32 lanes; the FP64 closed form per lane
-// only when a lane leaves the series range.
-GLAC_HD M3<f32x2> expm_morningstar_pair(const AH8<f32x2> &Z) {
-    const HQ<f32x2> Q = herm_from_ah(Z);
-    const HQ2<f32x2> S = herm_square(Q);
-    f32x2 c0, c1;
-    invariants(Q, S, c0, c1);
-    Cx<f32x2> f0, f1, f2;
-    if (c1.v.x < (float)GLAC_SERIES_C1_MAX && c1.v.y < (float)GLAC_SERIES_C1_MAX) {
-        ms_series(c0, c1, f0, f1, f2);
-    } else {
-        const ExpCoef a = ms_coefficients((double)c0.v.x, (double)c1.v.x);
-        const ExpCoef b = ms_coefficients((double)c0.v.y, (double)c1.v.y);
-        f0 = cx(f32x2((float)a.f0r, (float)b.f0r), f32x2((float)a.f0i, (float)b.f0i));
-        f1 = cx(f32x2((float)a.f1r, (float)b.f1r), f32x2((float)a.f1i, (float)b.f1i));
-        f2 = cx(f32x2((float)a.f2r, (float)b.f2r), f32x2((float)a.f2i, (float)b.f2i));
     }
     return ms_combine(Q, S, f0, f1, f2);
 }

@@ -4,60 +4,9 @@
 #include "kernels.cuh"
 
 #include <algorithm>
-#include <cstdlib>
 #include <stdexcept>
 
 namespace glac {
-
-// Minimum resident blocks per SM requested from ptxas (caps registers per thread).
-template <typename R> struct MinBlocks { static const int flow = 2, metro = 2, obs = 1; };
-template <> struct MinBlocks<double> { static const int flow = 3, metro = 3, obs = 1; };
-
-// lanes of a real: the physical sites a thread carries
-__device__ __forceinline__ double lane0(double v) { return v; }
-__device__ __forceinline__ double lane1(double) { return 0.0; }
-__device__ __forceinline__ double lane0(f32x2 v) { return (double)v.v.x; }
-__device__ __forceinline__ double lane1(f32x2 v) { return (double)v.v.y; }
-__device__ __forceinline__ double lanesum(double v) { return v; }
-__device__ __forceinline__ double lanesum(f32x2 v) { return (double)v.v.x + (double)v.v.y; }
-
-template <typename R> GLAC_HD R real_of(double v);
-template <> GLAC_HD double real_of<double>(double v) { return v; }
-template <> GLAC_HD f32x2 real_of<f32x2>(double v) { return f32x2((float)v); }
-
-// ---------------------------------------------------------------------------
-// Exponentials over R (Morningstar-Peardon by default; see expm.cuh)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ M3<f32x2> join_lanes(const M3<float> &a, const M3<float> &b) {
-    M3<f32x2> r;
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-        r.e[k].re = f32x2(a.e[k].re, b.e[k].re);
-        r.e[k].im = f32x2(a.e[k].im, b.e[k].im);
-    }
-    return r;
-}
-__device__ __forceinline__ AH8<float> lane_of(const AH8<f32x2> &Z, int lane) {
-    AH8<float> r;
-    r.a = lane ? Z.a.v.y : Z.a.v.x;
-    r.d = lane ? Z.d.v.y : Z.d.v.x;
-    r.b = cx(lane ? Z.b.re.v.y : Z.b.re.v.x, lane ? Z.b.im.v.y : Z.b.im.v.x);
-    r.c = cx(lane ? Z.c.re.v.y : Z.c.re.v.x, lane ? Z.c.im.v.y : Z.c.im.v.x);
-    r.e = cx(lane ? Z.e.re.v.y : Z.e.re.v.x, lane ? Z.e.im.v.y : Z.e.im.v.x);
-    return r;
-}
-
-template <typename R, int KIND> struct Expm;
-template <int KIND> struct Expm<double, KIND> {
-    static __device__ __forceinline__ M3<double> run(const AH8<double> &Z) { return expm<double>(KIND, Z); }
-};
-template <int KIND> struct Expm<f32x2, KIND> {
-    static __device__ __forceinline__ M3<f32x2> run(const AH8<f32x2> &Z) {
-        if (KIND == EXP_MORNINGSTAR) return expm_morningstar_pair(Z);
-        // alternates: per lane in scalar FP32
-        return join_lanes(expm<float>(KIND, lane_of(Z, 0)), expm<float>(KIND, lane_of(Z, 1)));
-    }
-};
 
 // ---------------------------------------------------------------------------
 // Flow stage (GLAC/flow/flow.cpp:43-73 with getActionDerivative,
@@ -71,43 +20,99 @@ template <int KIND> struct Expm<f32x2, KIND> {
 // together cover one region of the lattice for all planes, so the neighbour
 // links they share are read from HBM once and then hit in L2.
 // ---------------------------------------------------------------------------
-template <typename R, int KIND, int STAGE>
-__global__ void __launch_bounds__(128, MinBlocks<R>::flow)
-    k_flow_stage(Geom g, LinkField<R> in, LinkField<R> out, ForceField<R> zf, R alpha, R beta) {
+template <typename T, int KIND, int STAGE>
+__device__ __forceinline__ void flow_stage_body(const Geom &g, const LinkField<T> &in, const LinkField<T> &out,
+                                                const ForceField<T> &zf, T alpha, T beta) {
     const int plane = blockIdx.x & 7;
     const int s = (blockIdx.x >> 3) * blockDim.x + threadIdx.x;
     if (s >= g.Vh) return;
     const int mu = plane >> 1, p = plane & 1;
     const Site n = site_from_ps(g, p, s);
-    const M3<R> A = staple(in, g, n, p, mu);
-    const M3<R> U = in.load(mu, p, s);
-    const AH8<R> Z = project_ah(mul(U, A));
-    AH8<R> M;
+    M3<T> A = staple(in, g, n, p, mu);
+    const M3<T> U = in.load(mu, p, s);
+    const AH8<T> Z = project_ah(mul(U, A));
+    AH8<T> M;
     if (STAGE == 0) {
         M = ah_scale(alpha, Z);
         zf.store(mu, p, s, Z);
     } else {
-        const AH8<R> W = zf.load(mu, p, s);
+        const AH8<T> W = zf.load(mu, p, s);
         M = ah_axpby(alpha, Z, beta, W);
         if (STAGE == 1) zf.store(mu, p, s, M);
     }
-    out.store(mu, p, s, mul(Expm<R, KIND>::run(M), U));
+    out.store(mu, p, s, mul(expm<T>(KIND, M), U));
 }
 
-template <typename R>
-void launch_flow_stage(const Geom &g, const LinkField<R> &in, const LinkField<R> &out, const ForceField<R> &zf,
-                       int stage, int kind, double alpha, double beta, cudaStream_t st) {
+// One __global__ per register cap (REGS = 0: the compiler's own choice); the
+// autotuner picks among them per lattice.
+#define GLAC_FLOW_KERNEL(NAME, ATTR)                                                                      \
+    template <typename T, int KIND, int STAGE>                                                           \
+    __global__ void ATTR NAME(Geom g, LinkField<T> in, LinkField<T> out,                                 \
+                                                     ForceField<T> zf, T alpha, T beta) {                \
+        flow_stage_body<T, KIND, STAGE>(g, in, out, zf, alpha, beta);                                    \
+    }
+GLAC_FLOW_KERNEL(k_flow_stage, __launch_bounds__(128))
+GLAC_FLOW_KERNEL(k_flow_stage_r128, __maxnreg__(128))
+GLAC_FLOW_KERNEL(k_flow_stage_r96, __maxnreg__(96))
+GLAC_FLOW_KERNEL(k_flow_stage_r80, __maxnreg__(80))
+GLAC_FLOW_KERNEL(k_flow_stage_r72, __maxnreg__(72))
+#undef GLAC_FLOW_KERNEL
+
+// Launch-bound variants (minimum resident blocks of 128 threads per SM, i.e.
+// the register cap) that the autotuner chooses among; variant 0 is the default.
+// Register caps per variant ([fp64, fp32]; 0 = no cap, -1 = unused slot).
+const int kFlowRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 80, 72, 96}};
+const int kMetroRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 96, 80, 128}};
+const int kObsRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 128, -1, -1}};
+
+int num_variants(Family f, bool fp32) {
+    const int(*t)[kMaxVariants] = f == FAM_FLOW ? kFlowRegs : f == FAM_METRO ? kMetroRegs : kObsRegs;
+    int n = 0;
+    while (n < kMaxVariants && t[fp32 ? 1 : 0][n] >= 0) n++;
+    return n;
+}
+int variant_regs(Family f, bool fp32, int v) {
+    const int(*t)[kMaxVariants] = f == FAM_FLOW ? kFlowRegs : f == FAM_METRO ? kMetroRegs : kObsRegs;
+    return (v >= 0 && v < kMaxVariants) ? t[fp32 ? 1 : 0][v] : 0;
+}
+
+template <typename T, int KIND, int STAGE>
+static void flow_dispatch(int regs, dim3 grid, cudaStream_t st, const Geom &g, const LinkField<T> &in,
+                          const LinkField<T> &out, const ForceField<T> &zf, T a, T b) {
+    switch (regs) {
+    case 128: k_flow_stage_r128<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
+    case 96: k_flow_stage_r96<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
+    case 80: k_flow_stage_r80<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
+    case 72: k_flow_stage_r72<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
+    default: k_flow_stage<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
+    }
+}
+
+template <typename T>
+void launch_flow_stage(const Geom &g, const LinkField<T> &in, const LinkField<T> &out, const ForceField<T> &zf,
+                       int stage, int kind, double alpha, double beta, int variant, cudaStream_t st) {
     const dim3 grid(8 * ((g.Vh + 127) / 128));
-    const R a = real_of<R>(alpha), b = real_of<R>(beta);
+    const T a = (T)alpha, b = (T)beta;
+    const bool fp32 = sizeof(T) == 4;
+    if (kind == EXP_MORNINGSTAR) {
+        const int regs = variant_regs(FAM_FLOW, fp32, variant);
+        if (stage == 0) flow_dispatch<T, 0, 0>(regs, grid, st, g, in, out, zf, a, b);
+        else if (stage == 1) flow_dispatch<T, 0, 1>(regs, grid, st, g, in, out, zf, a, b);
+        else flow_dispatch<T, 0, 2>(regs, grid, st, g, in, out, zf, a, b);
+        return;
+    }
 #define GLAC_FLOW_CASE(K, S) \
-    if (kind == K && stage == S) { k_flow_stage<R, K, S><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); return; }
-    GLAC_FLOW_CASE(0, 0) GLAC_FLOW_CASE(0, 1) GLAC_FLOW_CASE(0, 2)
+    if (kind == K && stage == S) { k_flow_stage<T, K, S><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); return; }
     GLAC_FLOW_CASE(1, 0) GLAC_FLOW_CASE(1, 1) GLAC_FLOW_CASE(1, 2)
     GLAC_FLOW_CASE(2, 0) GLAC_FLOW_CASE(2, 1) GLAC_FLOW_CASE(2, 2)
     GLAC_FLOW_CASE(3, 0) GLAC_FLOW_CASE(3, 1) GLAC_FLOW_CASE(3, 2)
 #undef GLAC_FLOW_CASE
     throw std::invalid_argument("bad flow stage or exp kind");
 }
+template void launch_flow_stage<double>(const Geom &, const LinkField<double> &, const LinkField<double> &,
+                                        const ForceField<double> &, int, int, double, double, int, cudaStream_t);
+template void launch_flow_stage<float>(const Geom &, const LinkField<float> &, const LinkField<float> &,
+                                       const ForceField<float> &, int, int, double, double, int, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Checkerboard Metropolis sub-sweep over the links (mu, parity p).
@@ -120,10 +125,14 @@ void launch_flow_stage(const Geom &g, const LinkField<R> &in, const LinkField<R>
 // ReTr[(XU - U) A] = ReTr(X W) - ReTr(W); the products X U and X W are formed
 // only for accepted proposals.
 // Random numbers: Philox4x32-10, key = seed, counter = {2 hit + call,
-// mu V + lex, sweep, stream} (V, lex of the physical lattice): words 0-5 carry
-// twelve 16-bit uniforms (low half first) for R, S, T; words 6-7 the 53-bit
-// accept uniform; bit 0 of word 7 picks X or X^+.
+// mu V + lex, sweep, stream}: words 0-5 carry twelve 16-bit uniforms (low half
+// first) for R, S, T; words 6-7 the 53-bit accept uniform; bit 0 of word 7
+// picks X or X^+.
 // ---------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ T su_scalar(double v);
+template <> __device__ __forceinline__ double su_scalar<double>(double v) { return v; }
+template <> __device__ __forceinline__ float su_scalar<float>(double v) { return (float)v; }
+
 GLAC_HD double u_sym16(uint32_t h) { return ((double)h + 0.5) * (1.0 / 65536.0) - 0.5; }
 
 template <typename T>
@@ -138,15 +147,15 @@ __device__ __forceinline__ void su2_near_unity(T u0, T u1, T u2, T u3, T eps, T 
 }
 
 // X = R S T with the SU(2) elements [[x0 + i x3, x2 + i x1], [-x2 + i x1, x0 - i x3]]
-// embedded in the (12), (13), (23) blocks; zero blocks skipped.
-template <typename R>
-__device__ __forceinline__ M3<R> rst_matrix(const R r[4], const R s[4], const R t[4]) {
-    const Cx<R> r00 = cx(r[0], r[3]), r01 = cx(r[2], r[1]), r10 = cx(-r[2], r[1]), r11 = cx(r[0], -r[3]);
-    const Cx<R> s00 = cx(s[0], s[3]), s01 = cx(s[2], s[1]), s10 = cx(-s[2], s[1]), s11 = cx(s[0], -s[3]);
-    const Cx<R> t00 = cx(t[0], t[3]), t01 = cx(t[2], t[1]), t10 = cx(-t[2], t[1]), t11 = cx(t[0], -t[3]);
+// embedded in the (12), (13), (23) blocks; zero blocks skipped.  inverse -> X^+.
+template <typename T>
+__device__ __forceinline__ M3<T> rst_matrix(const T r[4], const T s[4], const T t[4], bool inverse) {
+    const Cx<T> r00 = cx(r[0], r[3]), r01 = cx(r[2], r[1]), r10 = cx(-r[2], r[1]), r11 = cx(r[0], -r[3]);
+    const Cx<T> s00 = cx(s[0], s[3]), s01 = cx(s[2], s[1]), s10 = cx(-s[2], s[1]), s11 = cx(s[0], -s[3]);
+    const Cx<T> t00 = cx(t[0], t[3]), t01 = cx(t[2], t[1]), t10 = cx(-t[2], t[1]), t11 = cx(t[0], -t[3]);
     // R S = [[r00 s00, r01, r00 s01], [r10 s00, r11, r10 s01], [s10, 0, s11]]
-    const Cx<R> a0 = r00 * s00, a2 = r00 * s01, b0 = r10 * s00, b2 = r10 * s01;
-    M3<R> X;
+    const Cx<T> a0 = r00 * s00, a2 = r00 * s01, b0 = r10 * s00, b2 = r10 * s01;
+    M3<T> X;
     X(0, 0) = a0;
     X(1, 0) = b0;
     X(2, 0) = s10;
@@ -156,14 +165,12 @@ __device__ __forceinline__ M3<R> rst_matrix(const R r[4], const R s[4], const R 
     X(0, 2) = cmac(r01 * t01, a2, t11);
     X(1, 2) = cmac(r11 * t01, b2, t11);
     X(2, 2) = s11 * t11;
-    return X;
+    return inverse ? dagger(X) : X;
 }
 
-// The SU(2) parameters (3 x 4 reals), inverse flag and accept uniform of one hit.
 template <typename T>
-__device__ __forceinline__ void draw_hit(uint32_t k0, uint32_t k1, uint32_t link_id, uint32_t sweep,
-                                         uint32_t stream_id, int hit, T eps, T sq1me, T su[3][4], bool &inverse,
-                                         double &r) {
+__device__ __forceinline__ void draw_proposal(uint32_t k0, uint32_t k1, uint32_t link_id, uint32_t sweep,
+                                              uint32_t stream_id, int hit, T eps, T sq1me, M3<T> &X, double &r) {
     uint32_t w[8];
 #pragma unroll
     for (int call = 0; call < 2; call++) {
@@ -171,6 +178,7 @@ __device__ __forceinline__ void draw_hit(uint32_t k0, uint32_t k1, uint32_t link
         U4 o = philox4x32_10(c, k0, k1);
         w[4 * call] = o.x; w[4 * call + 1] = o.y; w[4 * call + 2] = o.z; w[4 * call + 3] = o.w;
     }
+    T su[3][4];
 #pragma unroll
     for (int b = 0; b < 3; b++) {
         T u[4];
@@ -178,12 +186,23 @@ __device__ __forceinline__ void draw_hit(uint32_t k0, uint32_t k1, uint32_t link
         for (int c = 0; c < 4; c++) {
             const int k = 4 * b + c;
             const uint32_t word = w[k >> 1];
-            u[c] = (T)u_sym16((k & 1) ? (word >> 16) : (word & 0xFFFFu));
+            u[c] = su_scalar<T>(u_sym16((k & 1) ? (word >> 16) : (word & 0xFFFFu)));
         }
         su2_near_unity<T>(u[0], u[1], u[2], u[3], eps, sq1me, su[b]);
     }
-    inverse = (w[7] & 1u) == 0u;
+    X = rst_matrix<T>(su[0], su[1], su[2], (w[7] & 1u) == 0u);
     r = u_53(w[6], w[7]);
+}
+
+template <typename T> __device__ __forceinline__ double accept_weight(T dS);
+template <> __device__ __forceinline__ double accept_weight<double>(double dS) { return exp(-dS); }
+template <> __device__ __forceinline__ double accept_weight<float>(float dS) { return (double)expf(-dS); }
+
+template <typename T>
+__device__ __forceinline__ T delta_s(const M3<T> &U, const M3<T> &Up, const M3<T> &A, T mfac) {
+    M3<T> D = Up;
+    sub_from(D, U);
+    return retr_mul(D, A) * mfac;
 }
 
 __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned long long *dst) {
@@ -202,27 +221,25 @@ __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned lon
     }
 }
 
-// FP64: one link per thread
-__global__ void __launch_bounds__(128, MinBlocks<double>::metro)
-    k_metropolis_f64(Geom g, LinkField<double> L, int mu, int p, double mfac, double eps, double sq1me, int nhits,
-                     uint32_t k0, uint32_t k1, uint32_t sweep, uint32_t stream_id, unsigned long long *acc) {
+template <typename T>
+__device__ __forceinline__ void metropolis_body(const Geom &g, const LinkField<T> &L, int mu, int p, T mfac, T eps,
+                                                T sq1me, int nhits, uint32_t k0, uint32_t k1, uint32_t sweep,
+                                                uint32_t stream_id, unsigned long long *acc) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long na = 0;
     if (s < g.Vh) {
         const Site n = site_from_ps(g, p, s);
-        const M3<double> A = staple(L, g, n, p, mu);
-        M3<double> U = L.load_rw(mu, p, s);
-        M3<double> W = mul(U, A);
+        const M3<T> A = staple(L, g, n, p, mu);
+        M3<T> U = L.load_rw(mu, p, s);
+        M3<T> W = mul(U, A);
         const uint32_t link_id = (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex;
 #pragma unroll 1
         for (int h = 0; h < nhits; h++) {
-            double su[3][4], r;
-            bool inv;
-            draw_hit<double>(k0, k1, link_id, sweep, stream_id, h, eps, sq1me, su, inv, r);
-            M3<double> X = rst_matrix<double>(su[0], su[1], su[2]);
-            if (inv) X = dagger(X);
-            const double dS = (retr_mul(X, W) - retr(W)) * mfac;
-            if (exp(-dS) > r) {
+            M3<T> X;
+            double r;
+            draw_proposal<T>(k0, k1, link_id, sweep, stream_id, h, eps, sq1me, X, r);
+            const T dS = (retr_mul(X, W) - retr(W)) * mfac;
+            if (accept_weight<T>(dS) > r) {
                 U = mul(X, U);
                 W = mul(X, W);
                 na++;
@@ -233,141 +250,110 @@ __global__ void __launch_bounds__(128, MinBlocks<double>::metro)
     block_add_u64(na, acc);
 }
 
-// FP32: two links per thread (lane x at t, lane y at t + Nt/2), accepted per lane
-__device__ __forceinline__ void blend(M3<f32x2> &dst, const M3<f32x2> &src, bool x, bool y) {
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-        if (x) { dst.e[k].re.v.x = src.e[k].re.v.x; dst.e[k].im.v.x = src.e[k].im.v.x; }
-        if (y) { dst.e[k].re.v.y = src.e[k].re.v.y; dst.e[k].im.v.y = src.e[k].im.v.y; }
+#define GLAC_METRO_KERNEL(NAME, ATTR)                                                                        \
+    template <typename T>                                                                                  \
+    __global__ void ATTR NAME(Geom g, LinkField<T> L, int mu, int p, T mfac, T eps,                         \
+                                                     T sq1me, int nhits, uint32_t k0, uint32_t k1,          \
+                                                     uint32_t sweep, uint32_t stream_id,                    \
+                                                     unsigned long long *acc) {                             \
+        metropolis_body<T>(g, L, mu, p, mfac, eps, sq1me, nhits, k0, k1, sweep, stream_id, acc);           \
+    }
+GLAC_METRO_KERNEL(k_metropolis, __launch_bounds__(128))
+GLAC_METRO_KERNEL(k_metropolis_r128, __maxnreg__(128))
+GLAC_METRO_KERNEL(k_metropolis_r96, __maxnreg__(96))
+GLAC_METRO_KERNEL(k_metropolis_r80, __maxnreg__(80))
+#undef GLAC_METRO_KERNEL
+
+template <typename T>
+void launch_metropolis(const Geom &g, const LinkField<T> &L, int mu, int p, double beta, double eps, int nhits,
+                       uint64_t seed, uint32_t sweep, uint32_t stream_id, unsigned long long *acc, int variant,
+                       cudaStream_t st) {
+    const int B = 128;
+    const dim3 grid((g.Vh + B - 1) / B);
+    const T mfac = (T)(-beta / 3.0), e = (T)eps, sq = (T)sqrt(1.0 - eps * eps);
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    switch (variant_regs(FAM_METRO, sizeof(T) == 4, variant)) {
+    case 128: k_metropolis_r128<T><<<grid, B, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc); break;
+    case 96: k_metropolis_r96<T><<<grid, B, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc); break;
+    case 80: k_metropolis_r80<T><<<grid, B, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc); break;
+    default: k_metropolis<T><<<grid, B, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc); break;
     }
 }
-
-__global__ void __launch_bounds__(128, MinBlocks<f32x2>::metro)
-    k_metropolis_f32(Geom g, LinkField<f32x2> L, int mu, int p, float mfac, float eps, float sq1me, int nhits,
-                     uint32_t k0, uint32_t k1, uint32_t sweep, uint32_t stream_id, unsigned long long *acc) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long na = 0;
-    if (s < g.Vh) {
-        const Site n = site_from_ps(g, p, s);
-        const M3<f32x2> A = staple(L, g, n, p, mu);
-        M3<f32x2> U = L.load_rw(mu, p, s);
-        M3<f32x2> W = mul(U, A);
-        const uint32_t Vphys = (uint32_t)g.V * 2u;
-        const uint32_t id0 = (uint32_t)mu * Vphys + (uint32_t)n.lex;
-        const uint32_t id1 = id0 + (uint32_t)g.V;
-#pragma unroll 1
-        for (int h = 0; h < nhits; h++) {
-            float sa[3][4], sb[3][4];
-            bool inva, invb;
-            double ra, rb;
-            draw_hit<float>(k0, k1, id0, sweep, stream_id, h, eps, sq1me, sa, inva, ra);
-            draw_hit<float>(k0, k1, id1, sweep, stream_id, h, eps, sq1me, sb, invb, rb);
-            f32x2 r4[3][4];
-#pragma unroll
-            for (int b = 0; b < 3; b++)
-#pragma unroll
-                for (int c = 0; c < 4; c++) r4[b][c] = f32x2(sa[b][c], sb[b][c]);
-            M3<f32x2> X = rst_matrix<f32x2>(r4[0], r4[1], r4[2]);
-            if (inva || invb) blend(X, dagger(X), inva, invb);
-            const f32x2 dS = (retr_mul(X, W) - retr(W)) * f32x2(mfac);
-            const bool ax = (double)expf(-dS.v.x) > ra;
-            const bool ay = (double)expf(-dS.v.y) > rb;
-            if (ax || ay) {
-                blend(U, mul(X, U), ax, ay);
-                blend(W, mul(X, W), ax, ay);
-                na += (ax ? 1 : 0) + (ay ? 1 : 0);
-            }
-        }
-        L.store(mu, p, s, U);
-    }
-    block_add_u64(na, acc);
-}
-
-template <>
-void launch_metropolis<double>(const Geom &g, const LinkField<double> &L, int mu, int p, double beta, double eps,
-                               int nhits, uint64_t seed, uint32_t sweep, uint32_t stream_id,
-                               unsigned long long *acc, cudaStream_t st) {
-    k_metropolis_f64<<<(g.Vh + 127) / 128, 128, 0, st>>>(g, L, mu, p, -beta / 3.0, eps, sqrt(1.0 - eps * eps),
-                                                         nhits, (uint32_t)seed, (uint32_t)(seed >> 32), sweep,
-                                                         stream_id, acc);
-}
-template <>
-void launch_metropolis<f32x2>(const Geom &g, const LinkField<f32x2> &L, int mu, int p, double beta, double eps,
-                              int nhits, uint64_t seed, uint32_t sweep, uint32_t stream_id,
-                              unsigned long long *acc, cudaStream_t st) {
-    k_metropolis_f32<<<(g.Vh + 127) / 128, 128, 0, st>>>(g, L, mu, p, (float)(-beta / 3.0), (float)eps,
-                                                         (float)sqrt(1.0 - eps * eps), nhits, (uint32_t)seed,
-                                                         (uint32_t)(seed >> 32), sweep, stream_id, acc);
-}
+template void launch_metropolis<double>(const Geom &, const LinkField<double> &, int, int, double, double, int,
+                                        uint64_t, uint32_t, uint32_t, unsigned long long *, int, cudaStream_t);
+template void launch_metropolis<float>(const Geom &, const LinkField<float> &, int, int, double, double, int,
+                                       uint64_t, uint32_t, uint32_t, unsigned long long *, int, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Observables (GLAC/observables/mastersamplertopcxyz.cpp:236-384): per site,
 // for nu = 1..3 and its cyclic complement (rho, sigma), the clovers
 //   C = leaf1 - leaf2 + leaf3 - leaf4 projected to (C - C^+) - 1/3 i ImTr,
 // plaq += ReTr leaf1, q(t) -= ReTr(C_0nu C_rhosigma), E += ReTr(C C) for both.
-// Every block lies in one (t, parity) half-slice of the stored lattice, so its
-// sums are per-time-slice partials (two slices for two lanes); FP64 throughout
-// the reduction, fixed order.
+// Every block lies in one (t, parity) half-slice, so the block sums are
+// per-time-slice partials; FP64 throughout the reduction, fixed order.
 // ---------------------------------------------------------------------------
 ObsPlan make_obs_plan(const Geom &g) {
-    // a block covers Bv <= 32 sites of one (t, parity) half-slice, one warp per plane
     const int half_slice = g.N[0] * g.N[1] * g.N[2] / 2;
-    int best = 1;
-    for (int B = 1; B <= 32 && B <= half_slice; B++)
-        if (half_slice % B == 0) best = B;
+    int best = -1, best_score = 1 << 30;
+    for (int B = 1; B <= 256 && B <= half_slice; B++) {
+        if (half_slice % B) continue;
+        int score = (B % 32 == 0 ? 0 : 100000) + std::abs(B - 128);
+        if (score < best_score) { best_score = score; best = B; }
+    }
     ObsPlan pl;
     pl.Bv = best;
-    pl.B = 32;
+    pl.B = (best + 31) / 32 * 32;
     pl.nb = half_slice / best;
     pl.nblocks = g.N[3] * 2 * pl.nb;
     return pl;
 }
 
 // Clover of the (mu, nu) plane at n, projected: F = (C - C^+) - 1/3 i ImTr(C - C^+),
-// in the 8-real form; plaq = ReTr(leaf1).
-template <typename R>
-__device__ __forceinline__ AH8<R> clover_ah(const LinkField<R> &L, const Geom &g, const Site &n, int p, int mu,
-                                            int nu, R &plaq) {
+// returned in the 8-real form; *plaq = ReTr(leaf1).  Links are re-read from
+// L1/L2 rather than held, to keep register pressure low.
+template <typename T>
+__device__ __forceinline__ AH8<T> clover_ah(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu,
+                                            int nu, T &plaq) {
     const int q = p ^ 1;
-    const Nb n_0 = nb_self(n);
-    const Nb n_mup = nb_step(g, n, mu, +1);           // n+mu      (q)
-    const Nb n_nup = nb_step(g, n, nu, +1);           // n+nu      (q)
-    const Nb n_num = nb_step(g, n, nu, -1);           // n-nu      (q)
-    const Nb n_mum = nb_step(g, n, mu, -1);           // n-mu      (q)
-    const Nb n_pm = nb_step2(g, n, mu, +1, nu, -1);   // n+mu-nu   (p)
-    const Nb n_mm = nb_step2(g, n, mu, -1, nu, -1);   // n-mu-nu   (p)
-    const Nb n_mp = nb_step2(g, n, mu, -1, nu, +1);   // n-mu+nu   (p)
-    M3<R> C;
-    // compiler fences between the leaves keep their loads from all being
-    // hoisted to the top, which would multiply the live registers
+    const int s_n = n.lex >> 1;
+    const int s_mup = lex_step(g, n, mu, +1) >> 1;           // n+mu      (q)
+    const int s_nup = lex_step(g, n, nu, +1) >> 1;           // n+nu      (q)
+    const int s_num = lex_step(g, n, nu, -1) >> 1;           // n-nu      (q)
+    const int s_mum = lex_step(g, n, mu, -1) >> 1;           // n-mu      (q)
+    const int s_pm = lex_step2(g, n, mu, +1, nu, -1) >> 1;   // n+mu-nu   (p)
+    const int s_mm = lex_step2(g, n, mu, -1, nu, -1) >> 1;   // n-mu-nu   (p)
+    const int s_mp = lex_step2(g, n, mu, -1, nu, +1) >> 1;   // n-mu+nu   (p)
+    M3<T> C;
+    // compiler fences between the leaves keep their loads from being hoisted
+    // together, which would multiply the live registers
     {   // leaf1 = U_mu(n) U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+
-        const M3<R> P = mul(L.load(mu, p, n_0), L.load(nu, q, n_mup));
-        const M3<R> W = mul(L.load(nu, p, n_0), L.load(mu, q, n_nup));
+        const M3<T> P = mul(L.load(mu, p, s_n), L.load(nu, q, s_mup));
+        const M3<T> W = mul(L.load(nu, p, s_n), L.load(mu, q, s_nup));
         C = mul_nd(P, W);
         plaq = retr(C);
     }
     asm volatile("" ::: "memory");
     {   // leaf2 = U_mu(n) U_nu(n+mu-nu)^+ U_mu(n-nu)^+ U_nu(n-nu)
-        const M3<R> Y = mul(L.load(mu, q, n_num), L.load(nu, p, n_pm));
-        const M3<R> t = mul_nd(L.load(mu, p, n_0), Y);
-        sub_from(C, mul(t, L.load(nu, q, n_num)));
+        const M3<T> Y = mul(L.load(mu, q, s_num), L.load(nu, p, s_pm));
+        const M3<T> t = mul_nd(L.load(mu, p, s_n), Y);
+        sub_from(C, mul(t, L.load(nu, q, s_num)));
     }
     asm volatile("" ::: "memory");
     {   // leaf3 = U_mu(n-mu)^+ U_nu(n-mu-nu)^+ U_mu(n-mu-nu) U_nu(n-nu)
-        M3<R> t = mul_dd(L.load(mu, q, n_mum), L.load(nu, p, n_mm));
-        t = mul(t, L.load(mu, p, n_mm));
-        add_to(C, mul(t, L.load(nu, q, n_num)));
+        M3<T> t = mul_dd(L.load(mu, q, s_mum), L.load(nu, p, s_mm));
+        t = mul(t, L.load(mu, p, s_mm));
+        add_to(C, mul(t, L.load(nu, q, s_num)));
     }
     asm volatile("" ::: "memory");
     {   // leaf4 = U_mu(n-mu)^+ U_nu(n-mu) U_mu(n-mu+nu) U_nu(n)^+
-        M3<R> t = mul_dn(L.load(mu, q, n_mum), L.load(nu, q, n_mum));
-        t = mul(t, L.load(mu, p, n_mp));
-        sub_from(C, mul_nd(t, L.load(nu, p, n_0)));
+        M3<T> t = mul_dn(L.load(mu, q, s_mum), L.load(nu, q, s_mum));
+        t = mul(t, L.load(mu, p, s_mp));
+        sub_from(C, mul_nd(t, L.load(nu, p, s_n)));
     }
     // (C - C^+): diagonal 2 i Im C_ii, off-diagonal C_ij - conj(C_ji); then traceless
-    AH8<R> F;
-    const R two = real_of<R>(2.0);
-    const R tr = (C(0, 0).im + C(1, 1).im + C(2, 2).im) * real_of<R>(2.0 / 3.0);
+    AH8<T> F;
+    const T two = T(2);
+    const T tr = (C(0, 0).im + C(1, 1).im + C(2, 2).im) * T(2.0 / 3.0);
     F.a = two * C(0, 0).im - tr;
     F.d = two * C(1, 1).im - tr;
     F.b = cx(C(0, 1).re - C(1, 0).re, C(0, 1).im + C(1, 0).im);
@@ -378,11 +364,11 @@ __device__ __forceinline__ AH8<R> clover_ah(const LinkField<R> &L, const Geom &g
 
 // Re Tr(F G) for traceless anti-Hermitian F, G in the 8-real form:
 //   -[a a' + d d' + (a+d)(a'+d')] - 2 Re(b b'* + c c'* + e e'*)
-template <typename R>
-__device__ __forceinline__ R retr_ah(const AH8<R> &F, const AH8<R> &G) {
-    R diag = fmaR(F.a, G.a, F.d * G.d);
+template <typename T>
+__device__ __forceinline__ T retr_ah(const AH8<T> &F, const AH8<T> &G) {
+    T diag = fmaR(F.a, G.a, F.d * G.d);
     diag = fmaR(F.a + F.d, G.a + G.d, diag);
-    R off = fmaR(F.b.re, G.b.re, F.b.im * G.b.im);
+    T off = fmaR(F.b.re, G.b.re, F.b.im * G.b.im);
     off = fmaR(F.c.re, G.c.re, off);
     off = fmaR(F.c.im, G.c.im, off);
     off = fmaR(F.e.re, G.e.re, off);
@@ -396,67 +382,69 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
-// threadIdx.x: site in the block (Bv valid of 32), threadIdx.y: plane 0..5 =
-// (0,1) (0,2) (0,3) (2,3) (3,1) (1,2): planes y and y+3 pair up in q.
-template <typename R>
-__global__ void __launch_bounds__(192, MinBlocks<R>::obs)
-    k_observables(Geom g, LinkField<R> L, int nb, int Bv, double *partial) {
+template <typename T>
+__device__ __forceinline__ void observables_body(const Geom &g, const LinkField<T> &L, int nb, int Bv,
+                                                 double *partial) {
     const int b = blockIdx.x;
     const int t = b / (2 * nb);
     const int p = (b / nb) & 1;
     const int j = b % nb;
     const int half_slice = g.Vh / g.N[3];
-    const int tx = threadIdx.x, plane = threadIdx.y;
-    const bool valid = tx < Bv;
-    const int s = t * half_slice + j * Bv + (valid ? tx : 0);
-    int mu, nu;
-    if (plane < 3) { mu = 0; nu = plane + 1; }
-    else { mu = (plane - 3 + 1) % 3 + 1; nu = mu % 3 + 1; }
-    __shared__ AH8<R> shF[6][32];
-    double plaq = 0.0, en = 0.0, q0 = 0.0, q1 = 0.0;
-    AH8<R> F;
+    const bool valid = (int)threadIdx.x < Bv;
+    const int s = t * half_slice + j * Bv + (valid ? (int)threadIdx.x : 0);
+    double plaq = 0.0, en = 0.0, qt = 0.0;
+    const Site n = site_from_ps(g, p, s);
     if (valid) {
-        const Site n = site_from_ps(g, p, s);
-        R pl;
-        F = clover_ah(L, g, n, p, mu, nu, pl);
-        shF[plane][tx] = F;
-        plaq = lanesum(pl);
-        en = lanesum(retr_ah(F, F));
+#pragma unroll 1
+        for (int nu = 1; nu < 4; nu++) {
+            const int rho = nu % 3 + 1, sigma = rho % 3 + 1;
+            T pl1, pl2;
+            const AH8<T> F1 = clover_ah(L, g, n, p, 0, nu, pl1);
+            const AH8<T> F2 = clover_ah(L, g, n, p, rho, sigma, pl2);
+            plaq += (double)pl1 + (double)pl2;
+            qt -= (double)retr_ah(F1, F2);
+            en += (double)retr_ah(F1, F1) + (double)retr_ah(F2, F2);
+        }
     }
-    __syncthreads();
-    if (valid && plane < 3) {
-        const R q = retr_ah(F, shF[plane + 3][tx]);
-        q0 = -lane0(q);
-        q1 = -lane1(q);
-    }
-    // deterministic block reduction: warps (= planes) then planes in order
-    __shared__ double sh[kObsPartial][6];
+    // deterministic block reduction
+    __shared__ double sh[3][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     plaq = warp_sum_d(plaq);
     en = warp_sum_d(en);
-    q0 = warp_sum_d(q0);
-    q1 = warp_sum_d(q1);
-    if (tx == 0) { sh[0][plane] = plaq; sh[1][plane] = en; sh[2][plane] = q0; sh[3][plane] = q1; }
+    qt = warp_sum_d(qt);
+    if (lane == 0) { sh[0][wid] = plaq; sh[1][wid] = en; sh[2][wid] = qt; }
     __syncthreads();
-    if (plane == 0 && tx < kObsPartial) {
-        double a = 0.0;
-        for (int w = 0; w < 6; w++) a += sh[tx][w];
-        partial[kObsPartial * b + tx] = a;
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double a = 0.0, e = 0.0, q = 0.0;
+        for (int w = 0; w < nw; w++) { a += sh[0][w]; e += sh[1][w]; q += sh[2][w]; }
+        partial[3 * b] = a;
+        partial[3 * b + 1] = e;
+        partial[3 * b + 2] = q;
     }
 }
 
+#define GLAC_OBS_KERNEL(NAME, ATTR)                                                                      \
+    template <typename T>                                                                              \
+    __global__ void ATTR NAME(Geom g, LinkField<T> L, int nb, int Bv, double *partial) {               \
+        observables_body<T>(g, L, nb, Bv, partial);                                                    \
+    }
+GLAC_OBS_KERNEL(k_observables, __launch_bounds__(256))
+GLAC_OBS_KERNEL(k_observables_r128, __maxnreg__(128))
+GLAC_OBS_KERNEL(k_observables_r96, __maxnreg__(96))
+#undef GLAC_OBS_KERNEL
+
 // out = [plaq, topc, energy, topct[Nt]] with the reference's normalisations
-// (mastersamplertopcxyz.cpp:13-16, :363-383).  Physical slice t is lane t / NtS
-// of stored slice t % NtS.
-__global__ void k_obs_finalize(int NtS, int lanes, int nb, double Vphys, const double *partial, double *out) {
+// (mastersamplertopcxyz.cpp:13-16, :363-383).
+__global__ void k_obs_finalize(int Nt, int nb, int V, const double *partial, double *out) {
     __shared__ double sp[1024], se[1024], sq[1024];
-    const int Nt = NtS * lanes;
     for (int t = threadIdx.x; t < Nt; t += blockDim.x) {
-        const int ts = t % NtS, lane = t / NtS;
         double a = 0.0, e = 0.0, q = 0.0;
         for (int k = 0; k < 2 * nb; k++) {
-            const double *pp = partial + kObsPartial * ((size_t)ts * 2 * nb + k);
-            if (lane == 0) { a += pp[0]; e += pp[1]; }
-            q += pp[2 + lane];
+            const double *pp = partial + 3 * ((size_t)t * 2 * nb + k);
+            a += pp[0];
+            e += pp[1];
+            q += pp[2];
         }
         sp[t] = a; se[t] = e; sq[t] = q;
     }
@@ -464,48 +452,54 @@ __global__ void k_obs_finalize(int NtS, int lanes, int nb, double Vphys, const d
     if (threadIdx.x == 0) {
         const double qfac = 1.0 / (16 * 16 * M_PI * M_PI);
         double a = 0.0, e = 0.0, q = 0.0;
-        for (int t = 0; t < NtS; t++) { a += sp[t]; e += se[t]; }
-        for (int t = 0; t < Nt; t++) q += sq[t];
-        out[0] = a / (18.0 * Vphys);
+        for (int t = 0; t < Nt; t++) { a += sp[t]; e += se[t]; q += sq[t]; }
+        out[0] = a / (18.0 * (double)V);
         out[1] = q * qfac;
-        out[2] = e / Vphys;
+        out[2] = e / (double)V;
         for (int t = 0; t < Nt; t++) out[3 + t] = sq[t] * qfac;
     }
 }
 
-template <typename R>
-void launch_observables(const Geom &g, const LinkField<R> &L, const ObsPlan &plan, double *partial, double *out,
-                        cudaStream_t st) {
-    if (g.N[3] * g.lanes > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
-    k_observables<R><<<plan.nblocks, dim3(32, 6), 0, st>>>(g, L, plan.nb, plan.Bv, partial);
-    k_obs_finalize<<<1, 256, 0, st>>>(g.N[3], g.lanes, plan.nb, (double)g.V * g.lanes, partial, out);
+template <typename T>
+void launch_observables(const Geom &g, const LinkField<T> &L, const ObsPlan &plan, double *partial, double *out,
+                        int variant, cudaStream_t st) {
+    if (g.N[3] > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
+    switch (variant_regs(FAM_OBS, sizeof(T) == 4, variant)) {
+    case 128: k_observables_r128<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial); break;
+    case 96: k_observables_r96<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial); break;
+    default: k_observables<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial); break;
+    }
+    k_obs_finalize<<<1, 256, 0, st>>>(g.N[3], plan.nb, g.V, partial, out);
 }
+template void launch_observables<double>(const Geom &, const LinkField<double> &, const ObsPlan &, double *,
+                                         double *, int, cudaStream_t);
+template void launch_observables<float>(const Geom &, const LinkField<float> &, const ObsPlan &, double *,
+                                        double *, int, cudaStream_t);
 
 // ---------------------------------------------------------------------------
-// Start fields, reunitarisation, layout conversion: per physical link.
-// grid: x over the stored plane sites and lanes, y = plane (mu*2 + parity).
+// Start fields, reunitarisation, layout conversion
 // ---------------------------------------------------------------------------
-struct LinkRef {
-    int mu, p, s, lane, lex_phys;
-};
-// thread -> one physical link; false if out of range
-__device__ __forceinline__ bool link_of_thread(const Geom &g, LinkRef &r) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.Vh * g.lanes) return false;
-    r.lane = i >= g.Vh ? 1 : 0;
-    r.s = i - r.lane * g.Vh;
-    r.mu = blockIdx.y >> 1;
-    r.p = blockIdx.y & 1;
-    const Site n = site_from_ps(g, r.p, r.s);
-    r.lex_phys = n.lex + r.lane * g.V;
-    return true;
+template <typename T> __device__ __forceinline__ M3<T> to_t(const M3<double> &a) {
+    M3<T> r;
+#pragma unroll
+    for (int k = 0; k < 9; k++) { r.e[k].re = (T)a.e[k].re; r.e[k].im = (T)a.e[k].im; }
+    return r;
+}
+template <typename T> __device__ __forceinline__ M3<double> to_d(const M3<T> &a) {
+    M3<double> r;
+#pragma unroll
+    for (int k = 0; k < 9; k++) { r.e[k].re = (double)a.e[k].re; r.e[k].im = (double)a.e[k].im; }
+    return r;
 }
 
-template <typename R>
-__global__ void k_haar(Geom g, LinkField<R> L, uint32_t k0, uint32_t k1, uint32_t stream_id) {
-    LinkRef r;
-    if (!link_of_thread(g, r)) return;
-    const uint32_t link_id = (uint32_t)r.mu * (uint32_t)(g.V * g.lanes) + (uint32_t)r.lex_phys;
+// grid: x over Vh, y = mu*2 + parity
+template <typename T>
+__global__ void k_haar(Geom g, LinkField<T> L, uint32_t k0, uint32_t k1, uint32_t stream_id) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    const Site n = site_from_ps(g, p, s);
+    const uint32_t link_id = (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex;
     uint32_t w[20];
 #pragma unroll
     for (int call = 0; call < 5; call++) {
@@ -516,9 +510,9 @@ __global__ void k_haar(Geom g, LinkField<R> L, uint32_t k0, uint32_t k1, uint32_
     M3<double> Z;
 #pragma unroll
     for (int e = 0; e < 9; e++) {  // Box-Muller
-        const double u1 = ((double)w[2 * e] + 1.0) * 2.3283064365386963e-10;
-        const double u2 = (double)w[2 * e + 1] * 2.3283064365386963e-10;
-        const double rad = sqrt(-2.0 * log(u1));
+        double u1 = ((double)w[2 * e] + 1.0) * 2.3283064365386963e-10;
+        double u2 = (double)w[2 * e + 1] * 2.3283064365386963e-10;
+        double rad = sqrt(-2.0 * log(u1));
         double sn, cs;
         sincospi(2.0 * u2, &sn, &cs);
         Z.e[e] = cx(rad * cs, rad * sn);
@@ -552,14 +546,14 @@ __global__ void k_haar(Geom g, LinkField<R> L, uint32_t k0, uint32_t k1, uint32_
     const Cx<double> f = cx(cs, sn);
 #pragma unroll
     for (int e = 0; e < 9; e++) Z.e[e] = Z.e[e] * f;
-    L.store_lane(r.mu, r.p, r.s, r.lane, Z);
+    L.store(mu, p, s, to_t<T>(Z));
 }
 
-template <typename R>
-__global__ void k_cold(Geom g, LinkField<R> L) {
+template <typename T>
+__global__ void k_cold(Geom g, LinkField<T> L) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.Vh) return;
-    M3<R> I;
+    M3<T> I;
     set_identity(I);
     L.store(blockIdx.y >> 1, blockIdx.y & 1, s, I);
 }
@@ -591,126 +585,94 @@ __device__ __forceinline__ M3<double> reunit(M3<double> U) {
     return U;
 }
 
-template <typename R>
-__global__ void k_reunitarize(Geom g, LinkField<R> L) {
-    LinkRef r;
-    if (!link_of_thread(g, r)) return;
-    L.store_lane(r.mu, r.p, r.s, r.lane, reunit(L.load_lane(r.mu, r.p, r.s, r.lane)));
+template <typename T>
+__global__ void k_reunitarize(Geom g, LinkField<T> L) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    L.store(mu, p, s, to_t<T>(reunit(to_d(L.load_rw(mu, p, s)))));
 }
 
-// AoS host layout [mu][lex_phys][18] (FP64) <-> device layout
-template <typename R>
-__global__ void k_aos_to_soa(Geom g, const double *aos, LinkField<R> L) {
-    LinkRef r;
-    if (!link_of_thread(g, r)) return;
-    const double2 *src = reinterpret_cast<const double2 *>(aos + ((size_t)r.mu * g.V * g.lanes + r.lex_phys) * 18);
+// AoS host layout [mu][lex][18] (FP64) <-> SoA. grid: x over V, y = mu.
+template <typename T>
+__global__ void k_aos_to_soa(Geom g, const double *aos, LinkField<T> L) {
+    const int lex = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lex >= g.V) return;
+    const int mu = blockIdx.y;
+    const double2 *src = reinterpret_cast<const double2 *>(aos + ((size_t)mu * g.V + lex) * 18);
     M3<double> U;
 #pragma unroll
-    for (int k = 0; k < 9; k++) { const double2 v = src[k]; U.e[k] = cx(v.x, v.y); }
-    L.store_lane(r.mu, r.p, r.s, r.lane, U);
+    for (int k = 0; k < 9; k++) { double2 v = src[k]; U.e[k] = cx(v.x, v.y); }
+    const int p = parity_of_lex(g, lex);
+    L.store(mu, p, lex >> 1, to_t<T>(U));
 }
-template <typename R>
-__global__ void k_soa_to_aos(Geom g, LinkField<R> L, double *aos) {
-    LinkRef r;
-    if (!link_of_thread(g, r)) return;
-    const M3<double> U = L.load_lane(r.mu, r.p, r.s, r.lane);
-    double2 *dst = reinterpret_cast<double2 *>(aos + ((size_t)r.mu * g.V * g.lanes + r.lex_phys) * 18);
+template <typename T>
+__global__ void k_soa_to_aos(Geom g, LinkField<T> L, double *aos) {
+    const int lex = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lex >= g.V) return;
+    const int mu = blockIdx.y;
+    const int p = parity_of_lex(g, lex);
+    const M3<double> U = to_d(L.load_rw(mu, p, lex >> 1));
+    double2 *dst = reinterpret_cast<double2 *>(aos + ((size_t)mu * g.V + lex) * 18);
 #pragma unroll
     for (int k = 0; k < 9; k++) dst[k] = make_double2(U.e[k].re, U.e[k].im);
 }
-template <typename R>
-__global__ void k_copy_field(Geom g, LinkField<R> src, LinkField<R> dst) {
+template <typename T>
+__global__ void k_copy_field(Geom g, LinkField<T> src, LinkField<T> dst) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.Vh) return;
     const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
     dst.store(mu, p, s, src.load_rw(mu, p, s));
 }
 
-// max over links of |U U^+ - 1| (entrywise), FP64 result via atomicMax on the bit pattern.
-template <typename R>
-__global__ void k_unitarity(Geom g, LinkField<R> L, unsigned long long *out) {
-    LinkRef r;
-    if (!link_of_thread(g, r)) return;
-    const M3<double> U = L.load_lane(r.mu, r.p, r.s, r.lane);
-    const M3<double> P = mul_nd(U, U);
-    double m = 0.0;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            const double re = P(i, j).re - (i == j ? 1.0 : 0.0);
-            m = fmax(m, fmax(fabs(re), fabs(P(i, j).im)));
-        }
-    atomicMax(out, (unsigned long long)__double_as_longlong(m));
+template <typename T>
+void launch_haar(const Geom &g, const LinkField<T> &L, uint64_t seed, uint32_t stream_id, cudaStream_t st) {
+    k_haar<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L, (uint32_t)seed, (uint32_t)(seed >> 32), stream_id);
 }
-
-static dim3 link_grid(const Geom &g, int block) { return dim3((g.Vh * g.lanes + block - 1) / block, 8); }
-
-template <typename R>
-void launch_haar(const Geom &g, const LinkField<R> &L, uint64_t seed, uint32_t stream_id, cudaStream_t st) {
-    k_haar<R><<<link_grid(g, 128), 128, 0, st>>>(g, L, (uint32_t)seed, (uint32_t)(seed >> 32), stream_id);
+template <typename T>
+void launch_cold(const Geom &g, const LinkField<T> &L, cudaStream_t st) {
+    k_cold<T><<<dim3((g.Vh + 255) / 256, 8), 256, 0, st>>>(g, L);
 }
-template <typename R>
-void launch_cold(const Geom &g, const LinkField<R> &L, cudaStream_t st) {
-    k_cold<R><<<dim3((g.Vh + 255) / 256, 8), 256, 0, st>>>(g, L);
+template <typename T>
+void launch_reunitarize(const Geom &g, const LinkField<T> &L, cudaStream_t st) {
+    k_reunitarize<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L);
 }
-template <typename R>
-void launch_reunitarize(const Geom &g, const LinkField<R> &L, cudaStream_t st) {
-    k_reunitarize<R><<<link_grid(g, 128), 128, 0, st>>>(g, L);
+template <typename T>
+void launch_aos_to_soa(const Geom &g, const double *aos, const LinkField<T> &L, cudaStream_t st) {
+    k_aos_to_soa<T><<<dim3((g.V + 127) / 128, 4), 128, 0, st>>>(g, aos, L);
 }
-template <typename R>
-void launch_aos_to_soa(const Geom &g, const double *aos, const LinkField<R> &L, cudaStream_t st) {
-    k_aos_to_soa<R><<<link_grid(g, 128), 128, 0, st>>>(g, aos, L);
+template <typename T>
+void launch_soa_to_aos(const Geom &g, const LinkField<T> &L, double *aos, cudaStream_t st) {
+    k_soa_to_aos<T><<<dim3((g.V + 127) / 128, 4), 128, 0, st>>>(g, L, aos);
 }
-template <typename R>
-void launch_soa_to_aos(const Geom &g, const LinkField<R> &L, double *aos, cudaStream_t st) {
-    k_soa_to_aos<R><<<link_grid(g, 128), 128, 0, st>>>(g, L, aos);
-}
-template <typename R>
-void launch_copy_field(const Geom &g, const LinkField<R> &src, const LinkField<R> &dst, cudaStream_t st) {
-    k_copy_field<R><<<dim3((g.Vh + 255) / 256, 8), 256, 0, st>>>(g, src, dst);
-}
-template <typename R>
-void launch_max_unitarity_dev(const Geom &g, const LinkField<R> &L, double *out, cudaStream_t st) {
-    cudaMemsetAsync(out, 0, sizeof(double), st);
-    k_unitarity<R><<<link_grid(g, 128), 128, 0, st>>>(g, L, reinterpret_cast<unsigned long long *>(out));
+template <typename T>
+void launch_copy_field(const Geom &g, const LinkField<T> &src, const LinkField<T> &dst, cudaStream_t st) {
+    k_copy_field<T><<<dim3((g.Vh + 255) / 256, 8), 256, 0, st>>>(g, src, dst);
 }
 
 // ---------------------------------------------------------------------------
 // Test exports
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void store_aos_lane(double *out, size_t off, const M3<double> &A) {
-    double2 *dst = reinterpret_cast<double2 *>(out + off * 18);
-#pragma unroll
-    for (int k = 0; k < 9; k++) dst[k] = make_double2(A.e[k].re, A.e[k].im);
-}
-__device__ __forceinline__ M3<double> widen(const M3<double> &A, int) { return A; }
-__device__ __forceinline__ M3<double> widen(const M3<f32x2> &A, int lane) {
-    M3<double> r;
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-        r.e[k].re = lane ? (double)A.e[k].re.v.y : (double)A.e[k].re.v.x;
-        r.e[k].im = lane ? (double)A.e[k].im.v.y : (double)A.e[k].im.v.x;
-    }
-    return r;
-}
-
-// staples (force = 0) or flow forces as full matrices (force = 1)
-template <typename R>
-__global__ void k_staples_aos(Geom g, LinkField<R> L, double *out, int force) {
+template <typename T>
+__global__ void k_staples_aos(Geom g, LinkField<T> L, double *out, int force) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.Vh) return;
     const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
     const Site n = site_from_ps(g, p, s);
-    M3<R> A = staple(L, g, n, p, mu);
+    M3<T> A = staple(L, g, n, p, mu);
     if (force) A = ah_to_m3(project_ah(mul(L.load(mu, p, s), A)));
-    const size_t Vphys = (size_t)g.V * g.lanes;
-    for (int lane = 0; lane < g.lanes; lane++)
-        store_aos_lane(out, (size_t)mu * Vphys + n.lex + (size_t)lane * g.V, widen(A, lane));
+    const M3<double> Ad = to_d(A);
+    double2 *dst = reinterpret_cast<double2 *>(out + ((size_t)mu * g.V + n.lex) * 18);
+#pragma unroll
+    for (int k = 0; k < 9; k++) dst[k] = make_double2(Ad.e[k].re, Ad.e[k].im);
 }
-template <typename R>
-void launch_staples_aos(const Geom &g, const LinkField<R> &L, double *out, int force, cudaStream_t st) {
-    k_staples_aos<R><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L, out, force);
+template <typename T>
+void launch_staples_aos(const Geom &g, const LinkField<T> &L, double *out, cudaStream_t st) {
+    k_staples_aos<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L, out, 0);
+}
+template <typename T>
+void launch_force_aos(const Geom &g, const LinkField<T> &L, double *out, cudaStream_t st) {
+    k_staples_aos<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L, out, 1);
 }
 
 template <typename T>
@@ -743,18 +705,6 @@ void launch_exp_batch(int kind, const double *in, double *out, long n, cudaStrea
     k_exp_batch<T><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(kind, in, out, n);
 }
 
-template <typename T> __device__ __forceinline__ double accept_weight(T dS);
-template <> __device__ __forceinline__ double accept_weight<double>(double dS) { return exp(-dS); }
-template <> __device__ __forceinline__ double accept_weight<float>(float dS) { return (double)expf(-dS); }
-
-template <typename T>
-__device__ __forceinline__ T delta_s(const M3<T> &U, const M3<T> &Up, const M3<T> &A, T mfac) {
-    M3<T> D = Up;
-    sub_from(D, U);
-    return retr_mul(D, A) * mfac;
-}
-
-// the reference's accept step with given proposals (GLAC/system.cpp:340-352)
 template <typename T>
 __global__ void k_accept_fed(T mfac, long nlinks, int nhits, double *U, const double *A, const double *X,
                              const double *r, unsigned char *accept) {
@@ -789,34 +739,47 @@ void launch_delta_s(double beta, long n, const double *U, const double *Up, cons
     k_delta_s<T><<<(unsigned)((n + 127) / 128), 128, 0, st>>>((T)(-beta / 3.0), n, U, Up, A, out);
 }
 
-// ---------------------------------------------------------------------------
-// Explicit instantiations
-// ---------------------------------------------------------------------------
-#define GLAC_INST_FIELD(R)                                                                                      \
-    template void launch_flow_stage<R>(const Geom &, const LinkField<R> &, const LinkField<R> &,                \
-                                       const ForceField<R> &, int, int, double, double, cudaStream_t);          \
-    template void launch_observables<R>(const Geom &, const LinkField<R> &, const ObsPlan &, double *, double *, \
-                                        cudaStream_t);                                                          \
-    template void launch_haar<R>(const Geom &, const LinkField<R> &, uint64_t, uint32_t, cudaStream_t);         \
-    template void launch_cold<R>(const Geom &, const LinkField<R> &, cudaStream_t);                             \
-    template void launch_reunitarize<R>(const Geom &, const LinkField<R> &, cudaStream_t);                      \
-    template void launch_aos_to_soa<R>(const Geom &, const double *, const LinkField<R> &, cudaStream_t);       \
-    template void launch_soa_to_aos<R>(const Geom &, const LinkField<R> &, double *, cudaStream_t);             \
-    template void launch_copy_field<R>(const Geom &, const LinkField<R> &, const LinkField<R> &, cudaStream_t); \
-    template void launch_staples_aos<R>(const Geom &, const LinkField<R> &, double *, int, cudaStream_t);       \
-    template void launch_max_unitarity_dev<R>(const Geom &, const LinkField<R> &, double *, cudaStream_t);
-GLAC_INST_FIELD(double)
-GLAC_INST_FIELD(f32x2)
-#undef GLAC_INST_FIELD
+// max over links of |U U^+ - 1| (entrywise), FP64 result in out[0] via atomicMax on the bit pattern.
+template <typename T>
+__global__ void k_unitarity(Geom g, LinkField<T> L, unsigned long long *out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    const M3<double> U = to_d(L.load_rw(mu, p, s));
+    const M3<double> P = mul_nd(U, U);
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            double re = P(i, j).re - (i == j ? 1.0 : 0.0);
+            m = fmax(m, fmax(fabs(re), fabs(P(i, j).im)));
+        }
+    atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+template <typename T>
+void launch_max_unitarity_dev(const Geom &g, const LinkField<T> &L, double *out, cudaStream_t st) {
+    cudaMemsetAsync(out, 0, sizeof(double), st);
+    k_unitarity<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L, reinterpret_cast<unsigned long long *>(out));
+}
 
-#define GLAC_INST_MAT(T)                                                                                 \
-    template void launch_exp_batch<T>(int, const double *, double *, long, cudaStream_t);                \
-    template void launch_accept_fed<T>(double, long, int, double *, const double *, const double *,      \
-                                       const double *, unsigned char *, cudaStream_t);                   \
-    template void launch_delta_s<T>(double, long, const double *, const double *, const double *, double *, \
+#define GLAC_INST(T)                                                                                             \
+    template void launch_haar<T>(const Geom &, const LinkField<T> &, uint64_t, uint32_t, cudaStream_t);          \
+    template void launch_cold<T>(const Geom &, const LinkField<T> &, cudaStream_t);                              \
+    template void launch_reunitarize<T>(const Geom &, const LinkField<T> &, cudaStream_t);                       \
+    template void launch_aos_to_soa<T>(const Geom &, const double *, const LinkField<T> &, cudaStream_t);        \
+    template void launch_soa_to_aos<T>(const Geom &, const LinkField<T> &, double *, cudaStream_t);              \
+    template void launch_copy_field<T>(const Geom &, const LinkField<T> &, const LinkField<T> &, cudaStream_t);  \
+    template void launch_staples_aos<T>(const Geom &, const LinkField<T> &, double *, cudaStream_t);             \
+    template void launch_force_aos<T>(const Geom &, const LinkField<T> &, double *, cudaStream_t);               \
+    template void launch_exp_batch<T>(int, const double *, double *, long, cudaStream_t);                        \
+    template void launch_accept_fed<T>(double, long, int, double *, const double *, const double *,              \
+                                       const double *, unsigned char *, cudaStream_t);                           \
+    template void launch_max_unitarity_dev<T>(const Geom &, const LinkField<T> &, double *, cudaStream_t);      \
+    template void launch_delta_s<T>(double, long, const double *, const double *, const double *, double *,     \
                                     cudaStream_t);
-GLAC_INST_MAT(double)
-GLAC_INST_MAT(float)
-#undef GLAC_INST_MAT
+GLAC_INST(double)
+GLAC_INST(float)
+#undef GLAC_INST
 
 }  // namespace glac

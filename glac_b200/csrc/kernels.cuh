@@ -1,8 +1,4 @@
 // Device kernels of the hot path and their host-side launchers.
-//
-// Kernels are written once over the real type R: double for the FP64 path
-// (one lattice site per thread) and f32x2 for the FP32 path (two lattice
-// sites per thread, one per FP32 lane, see lattice.cuh).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -16,26 +12,31 @@ namespace glac {
 // getActionDerivative :55-86):
 //   sum_{nu != mu}  U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+  +  U_nu(n+mu-nu)^+ U_mu(n-nu)^+ U_nu(n-nu)
 // n has parity p; n +- nu and n + mu have parity 1-p, n + mu - nu has parity p.
-template <typename R>
-__device__ __forceinline__ M3<R> staple(const LinkField<R> &L, const Geom &g, const Site &n, int p, int mu) {
-    M3<R> A;
+template <typename T>
+__device__ __forceinline__ M3<T> staple(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu) {
+    M3<T> A;
     set_zero(A);
     const int q = p ^ 1;
-    const Nb n_mu = nb_step(g, n, mu, +1);
-    const Nb n_0 = nb_self(n);
+    const int s_mu = lex_step(g, n, mu, +1) >> 1;
 #pragma unroll 1
     for (int nu = 0; nu < 4; nu++) {
         if (nu == mu) continue;
-        const Nb n_nup = nb_step(g, n, nu, +1);
-        const Nb n_num = nb_step(g, n, nu, -1);
-        const Nb n_diag = nb_step2(g, n, mu, +1, nu, -1);
+        const int s_nup = lex_step(g, n, nu, +1) >> 1;
+        const int s_num = lex_step(g, n, nu, -1) >> 1;
+        const int s_diag = lex_step2(g, n, mu, +1, nu, -1) >> 1;
         {
-            const M3<R> t = mul_nd(L.load(nu, q, n_mu), L.load(mu, q, n_nup));
-            acc_mul_nd(A, t, L.load(nu, p, n_0));
+            M3<T> a = L.load(nu, q, s_mu);
+            M3<T> b = L.load(mu, q, s_nup);
+            M3<T> t = mul_nd(a, b);
+            M3<T> c = L.load(nu, p, n.lex >> 1);
+            acc_mul_nd(A, t, c);
         }
         {
-            const M3<R> t = mul_dd(L.load(nu, p, n_diag), L.load(mu, q, n_num));
-            acc_mul(A, t, L.load(nu, q, n_num));
+            M3<T> a = L.load(nu, p, s_diag);
+            M3<T> b = L.load(mu, q, s_num);
+            M3<T> t = mul_dd(a, b);
+            M3<T> c = L.load(nu, q, s_num);
+            acc_mul(A, t, c);
         }
     }
     return A;
@@ -48,39 +49,44 @@ struct ObsPlan {
     int Bv;       // sites per block; divides the parity half of a time slice
     int B;        // threads per block (Bv rounded up to a whole warp)
     int nb;       // blocks per (t, parity)
-    int nblocks;  // Nt_stored * 2 * nb
+    int nblocks;  // Nt * 2 * nb
 };
 ObsPlan make_obs_plan(const Geom &g);
-constexpr int kObsPartial = 4;  // plaq, energy, q(lane 0), q(lane 1) per block
 
-template <typename R>
-void launch_flow_stage(const Geom &g, const LinkField<R> &in, const LinkField<R> &out, const ForceField<R> &zf,
-                       int stage, int kind, double alpha, double beta, cudaStream_t st);
-template <typename R>
-void launch_metropolis(const Geom &g, const LinkField<R> &L, int mu, int p, double beta, double eps, int nhits,
-                       uint64_t seed, uint32_t sweep, uint32_t stream_id, unsigned long long *acc, cudaStream_t st);
-template <typename R>
-void launch_observables(const Geom &g, const LinkField<R> &L, const ObsPlan &plan, double *partial,
-                        double *out, cudaStream_t st);
-template <typename R>
-void launch_haar(const Geom &g, const LinkField<R> &L, uint64_t seed, uint32_t stream_id, cudaStream_t st);
-template <typename R>
-void launch_cold(const Geom &g, const LinkField<R> &L, cudaStream_t st);
-template <typename R>
-void launch_reunitarize(const Geom &g, const LinkField<R> &L, cudaStream_t st);
-template <typename R>
-void launch_aos_to_soa(const Geom &g, const double *aos, const LinkField<R> &L, cudaStream_t st);
-template <typename R>
-void launch_soa_to_aos(const Geom &g, const LinkField<R> &L, double *aos, cudaStream_t st);
-template <typename R>
-void launch_copy_field(const Geom &g, const LinkField<R> &src, const LinkField<R> &dst, cudaStream_t st);
+// Kernel families with launch variants chosen by the autotuner (glac_autotune).
+enum Family { FAM_FLOW = 0, FAM_METRO = 1, FAM_OBS = 2 };
+constexpr int kMaxVariants = 4;
+int num_variants(Family f, bool fp32);
+int variant_regs(Family f, bool fp32, int v);  // register cap of a variant (0 = none)
+
+template <typename T>
+void launch_flow_stage(const Geom &g, const LinkField<T> &in, const LinkField<T> &out, const ForceField<T> &zf,
+                       int stage, int kind, double alpha, double beta, int variant, cudaStream_t st);
+template <typename T>
+void launch_metropolis(const Geom &g, const LinkField<T> &L, int mu, int p, double beta, double eps, int nhits,
+                       uint64_t seed, uint32_t sweep, uint32_t stream_id, unsigned long long *acc, int variant,
+                       cudaStream_t st);
+template <typename T>
+void launch_observables(const Geom &g, const LinkField<T> &L, const ObsPlan &plan, double *partial,
+                        double *out, int variant, cudaStream_t st);
+template <typename T>
+void launch_haar(const Geom &g, const LinkField<T> &L, uint64_t seed, uint32_t stream_id, cudaStream_t st);
+template <typename T>
+void launch_cold(const Geom &g, const LinkField<T> &L, cudaStream_t st);
+template <typename T>
+void launch_reunitarize(const Geom &g, const LinkField<T> &L, cudaStream_t st);
+template <typename T>
+void launch_aos_to_soa(const Geom &g, const double *aos, const LinkField<T> &L, cudaStream_t st);
+template <typename T>
+void launch_soa_to_aos(const Geom &g, const LinkField<T> &L, double *aos, cudaStream_t st);
+template <typename T>
+void launch_copy_field(const Geom &g, const LinkField<T> &src, const LinkField<T> &dst, cudaStream_t st);
 
 // test exports: outputs in the reference's host layout [mu][lex][18] (FP64)
-template <typename R>
-void launch_staples_aos(const Geom &g, const LinkField<R> &L, double *out, int force, cudaStream_t st);
-template <typename R>
-void launch_max_unitarity_dev(const Geom &g, const LinkField<R> &L, double *out, cudaStream_t st);
-// single matrices (T = double or float)
+template <typename T>
+void launch_staples_aos(const Geom &g, const LinkField<T> &L, double *out, cudaStream_t st);
+template <typename T>
+void launch_force_aos(const Geom &g, const LinkField<T> &L, double *out, cudaStream_t st);
 template <typename T>
 void launch_exp_batch(int kind, const double *in, double *out, long n, cudaStream_t st);
 template <typename T>
@@ -89,5 +95,7 @@ void launch_accept_fed(double beta, long nlinks, int nhits, double *U, const dou
 template <typename T>
 void launch_delta_s(double beta, long n, const double *U, const double *Up, const double *A, double *out,
                     cudaStream_t st);
+template <typename T>
+void launch_max_unitarity_dev(const Geom &g, const LinkField<T> &L, double *out, cudaStream_t st);
 
 }  // namespace glac

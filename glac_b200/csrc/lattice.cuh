@@ -1,26 +1,23 @@
 // Lattice geometry, the HBM layout of gauge fields, and the Philox streams.
 //
-// Layout.  Sites are split by parity (even/odd planes of Vh = V/2 sites, site
-// index s = lex >> 1 with lex = x + Nx(y + Ny(z + Nz t)), the reference's order,
-// GLAC/parallelization/index.h:32-35; Nx must be even), per link direction mu:
-// plane = mu*2 + parity.  Inside a plane the sites form tiles of 32; a tile
-// holds each 16-byte chunk of its 32 links contiguously, so a warp reading 32
-// consecutive sites of one chunk issues fully coalesced 128-bit loads, and the
-// chunks of a link sit at fixed 512-byte offsets from one base address.
-//
-//   FP64 (real type double): the full lattice; 9 double2 chunks per link,
-//     chunk k = complex element k (row-major).
-//   FP32 (real type f32x2): the lattice is cut into two halves along t; the
-//     stored lattice has Nt/2 time slices and every stored site carries two
-//     lattice sites in the two FP32 lanes: lane x = (x,y,z,t), lane y =
-//     (x,y,z,t + Nt/2) (same parity when Nt/2 is even).  9 float4 chunks per
-//     site pair, chunk k = (re_k lane x, re_k lane y, im_k lane x, im_k lane y),
-//     i.e. exactly one packed f32x2 complex number, so all FP32 arithmetic is
-//     fma.rn.f32x2 with no repacking.  Stepping across the cut in t swaps the
-//     lanes of the loaded pair.
-//
+// Layout (even/odd split, arrays of 32-site tiles): a field of 4 link
+// directions over V = Nx Ny Nz Nt sites is stored per (mu, parity) plane of
+// Vh = V/2 sites.  Inside a plane the sites form tiles of 32 (Vh32 = Vh rounded
+// up to 32); a tile holds each 16-byte chunk of its 32 links contiguously, so a
+// warp reading 32 consecutive sites of one chunk issues fully coalesced 128-bit
+// loads, and the chunks of one link sit at fixed 512-byte offsets from one base
+// address (no per-chunk address registers):
+//   FP64: 9 double2 chunks (chunk k = complex element k, row-major)
+//         addr = plane*9*Vh32 + (s>>5)*9*32 + k*32 + (s&31)
+//   FP32: 4 float4 chunks (complex elements 2k, 2k+1) in tiles, plus element 8
+//         as a plain float2 array:  addr4 = plane*4*Vh32 + (s>>5)*4*32 + k*32 + (s&31),
+//         addr2 = plane*Vh + s
+//   plane = mu*2 + parity.
+// The site index inside a parity plane is s = lex >> 1 with
+// lex = x + Nx(y + Ny(z + Nz t)), the reference's site order
+// (GLAC/parallelization/index.h:32-35); Nx must be even.
 // Traceless anti-Hermitian flow forces use 8 reals per link (a, d, b, c, e) in
-// the same tiling: FP64 4 double2 chunks, FP32 4 float4 chunks.
+// the same tiling: FP64 4 double2 chunks, FP32 2 float4 chunks.
 #pragma once
 
 #include <stdint.h>
@@ -47,23 +44,17 @@ GLAC_HD uint32_t fdiv(uint32_t n, const FastDiv &f) {
 #endif
 }
 
-// Geometry of the stored lattice: for lanes == 2 (FP32) its t extent is half
-// the physical one and the physical lattice is twice its volume.
 struct Geom {
     int N[4];
     int Nxh;
     int Vh;
     int V;
     int stride[4];  // lexicographic strides 1, Nx, Nx Ny, Nx Ny Nz
-    int lanes;      // 1 (FP64) or 2 (FP32, lane y = t + N[3])
     FastDiv div_xh, div_y, div_z;
 };
 
-// dims are the physical extents; lanes = 2 halves Nt.
-inline Geom make_geom(const int dims[4], int lanes = 1) {
-    int N[4] = {dims[0], dims[1], dims[2], dims[3] / lanes};
+inline Geom make_geom(const int N[4]) {
     Geom g;
-    g.lanes = lanes;
     for (int d = 0; d < 4; d++) g.N[d] = N[d];
     g.Nxh = N[0] / 2;
     g.V = N[0] * N[1] * N[2] * N[3];
@@ -99,44 +90,23 @@ GLAC_HD Site site_from_ps(const Geom &g, int p, int s) {
     return st;
 }
 
-// A neighbour: its index in the parity plane and whether the step crossed the
-// t cut of a two-lane lattice (then the lanes of what is loaded are swapped).
-struct Nb {
-    int s;
-    int swap;
-};
-
-// n + a e_d (a = +1 or -1), periodic
-GLAC_HD Nb nb_step(const Geom &g, const Site &n, int d, int a) {
-    const int cd = n.c[d];
+// lexicographic index of n + a e_d (a = +1 or -1), periodic
+GLAC_HD int lex_step(const Geom &g, const Site &n, int d, int a) {
+    int cd = n.c[d];
     int off;
-    bool wrap;
-    if (a > 0) { wrap = cd == g.N[d] - 1; off = wrap ? -(g.N[d] - 1) * g.stride[d] : g.stride[d]; }
-    else { wrap = cd == 0; off = wrap ? (g.N[d] - 1) * g.stride[d] : -g.stride[d]; }
-    Nb r;
-    r.s = (n.lex + off) >> 1;
-    r.swap = (g.lanes == 2 && d == 3 && wrap) ? 1 : 0;
-    return r;
+    if (a > 0) off = (cd == g.N[d] - 1) ? -(g.N[d] - 1) * g.stride[d] : g.stride[d];
+    else off = (cd == 0) ? (g.N[d] - 1) * g.stride[d] : -g.stride[d];
+    return n.lex + off;
 }
-// n + a e_d + b e_e (d != e)
-GLAC_HD Nb nb_step2(const Geom &g, const Site &n, int d, int a, int e, int b) {
-    const int cd = n.c[d], ce = n.c[e];
+// lexicographic index of n + a e_d + b e_e (d != e)
+GLAC_HD int lex_step2(const Geom &g, const Site &n, int d, int a, int e, int b) {
+    int cd = n.c[d], ce = n.c[e];
     int off;
-    bool wd, we;
-    if (a > 0) { wd = cd == g.N[d] - 1; off = wd ? -(g.N[d] - 1) * g.stride[d] : g.stride[d]; }
-    else { wd = cd == 0; off = wd ? (g.N[d] - 1) * g.stride[d] : -g.stride[d]; }
-    if (b > 0) { we = ce == g.N[e] - 1; off += we ? -(g.N[e] - 1) * g.stride[e] : g.stride[e]; }
-    else { we = ce == 0; off += we ? (g.N[e] - 1) * g.stride[e] : -g.stride[e]; }
-    Nb r;
-    r.s = (n.lex + off) >> 1;
-    r.swap = (g.lanes == 2 && ((d == 3 && wd) || (e == 3 && we))) ? 1 : 0;
-    return r;
-}
-GLAC_HD Nb nb_self(const Site &n) {
-    Nb r;
-    r.s = n.lex >> 1;
-    r.swap = 0;
-    return r;
+    if (a > 0) off = (cd == g.N[d] - 1) ? -(g.N[d] - 1) * g.stride[d] : g.stride[d];
+    else off = (cd == 0) ? (g.N[d] - 1) * g.stride[d] : -g.stride[d];
+    if (b > 0) off += (ce == g.N[e] - 1) ? -(g.N[e] - 1) * g.stride[e] : g.stride[e];
+    else off += (ce == 0) ? (g.N[e] - 1) * g.stride[e] : -g.stride[e];
+    return n.lex + off;
 }
 
 GLAC_HD int parity_of_lex(const Geom &g, int lex) {
@@ -155,15 +125,7 @@ GLAC_HD int parity_of_lex(const Geom &g, int lex) {
 // ---------------------------------------------------------------------------
 GLAC_HD int round32(int v) { return (v + 31) & ~31; }
 
-GLAC_HD f32x2 lane_swap(f32x2 a) { return f32x2(a.v.y, a.v.x); }
-GLAC_HD M3<f32x2> lane_swap(const M3<f32x2> &A) {
-    M3<f32x2> B;
-#pragma unroll
-    for (int k = 0; k < 9; k++) { B.e[k].re = lane_swap(A.e[k].re); B.e[k].im = lane_swap(A.e[k].im); }
-    return B;
-}
-
-template <typename R> struct LinkField;
+template <typename T> struct LinkField;
 
 template <> struct LinkField<double> {
     double2 *p;
@@ -171,7 +133,6 @@ template <> struct LinkField<double> {
     GLAC_HD size_t base(int mu, int par, int s) const {
         return (size_t)(mu * 2 + par) * 9 * (size_t)Vh32 + (size_t)(s >> 5) * 288 + (size_t)(s & 31);
     }
-    __device__ __forceinline__ M3<double> load(int mu, int par, Nb nb) const { return load(mu, par, nb.s); }
     __device__ __forceinline__ M3<double> load(int mu, int par, int s) const {
         const double2 *b = p + base(mu, par, s);
         M3<double> U;
@@ -197,74 +158,50 @@ template <> struct LinkField<double> {
 #pragma unroll
         for (int k = 0; k < 9; k++) b[32 * k] = make_double2(U.e[k].re, U.e[k].im);
     }
-    // one lattice site (lane ignored for FP64)
-    __device__ __forceinline__ M3<double> load_lane(int mu, int par, int s, int) const { return load_rw(mu, par, s); }
-    __device__ __forceinline__ void store_lane(int mu, int par, int s, int, const M3<double> &U) const {
-        store(mu, par, s, U);
-    }
 };
 
-// FP32: site pairs in packed lanes (lane x: t < Nt/2, lane y: t + Nt/2)
-template <> struct LinkField<f32x2> {
-    float4 *p;
+template <> struct LinkField<float> {
+    float4 *p4;
+    float2 *p2;
     int Vh, Vh32;
-    GLAC_HD size_t base(int mu, int par, int s) const {
-        return (size_t)(mu * 2 + par) * 9 * (size_t)Vh32 + (size_t)(s >> 5) * 288 + (size_t)(s & 31);
+    GLAC_HD size_t base4(int mu, int par, int s) const {
+        return (size_t)(mu * 2 + par) * 4 * (size_t)Vh32 + (size_t)(s >> 5) * 128 + (size_t)(s & 31);
     }
-    __device__ __forceinline__ M3<f32x2> load(int mu, int par, int s) const {
-        const float4 *b = p + base(mu, par, s);
-        M3<f32x2> U;
+    GLAC_HD size_t at2(int mu, int par, int s) const { return ((size_t)(mu * 2 + par)) * (size_t)Vh + (size_t)s; }
+    __device__ __forceinline__ M3<float> load(int mu, int par, int s) const {
+        const float4 *b = p4 + base4(mu, par, s);
+        M3<float> U;
 #pragma unroll
-        for (int k = 0; k < 9; k++) {
-            const float4 v = __ldg(b + 32 * k);
-            U.e[k].re = f32x2(v.x, v.y);
-            U.e[k].im = f32x2(v.z, v.w);
+        for (int k = 0; k < 4; k++) {
+            float4 v = __ldg(b + 32 * k);
+            U.e[2 * k].re = v.x; U.e[2 * k].im = v.y; U.e[2 * k + 1].re = v.z; U.e[2 * k + 1].im = v.w;
         }
+        float2 w = __ldg(p2 + at2(mu, par, s));
+        U.e[8].re = w.x; U.e[8].im = w.y;
         return U;
     }
-    __device__ __forceinline__ M3<f32x2> load(int mu, int par, Nb nb) const {
-        const M3<f32x2> U = load(mu, par, nb.s);
-        return nb.swap ? lane_swap(U) : U;
-    }
-    __device__ __forceinline__ M3<f32x2> load_rw(int mu, int par, int s) const {
-        const float4 *b = p + base(mu, par, s);
-        M3<f32x2> U;
+    __device__ __forceinline__ M3<float> load_rw(int mu, int par, int s) const {
+        const float4 *b = p4 + base4(mu, par, s);
+        M3<float> U;
 #pragma unroll
-        for (int k = 0; k < 9; k++) {
-            const float4 v = b[32 * k];
-            U.e[k].re = f32x2(v.x, v.y);
-            U.e[k].im = f32x2(v.z, v.w);
+        for (int k = 0; k < 4; k++) {
+            float4 v = b[32 * k];
+            U.e[2 * k].re = v.x; U.e[2 * k].im = v.y; U.e[2 * k + 1].re = v.z; U.e[2 * k + 1].im = v.w;
         }
+        float2 w = p2[at2(mu, par, s)];
+        U.e[8].re = w.x; U.e[8].im = w.y;
         return U;
     }
-    __device__ __forceinline__ void store(int mu, int par, int s, const M3<f32x2> &U) const {
-        float4 *b = p + base(mu, par, s);
+    __device__ __forceinline__ void store(int mu, int par, int s, const M3<float> &U) const {
+        float4 *b = p4 + base4(mu, par, s);
 #pragma unroll
-        for (int k = 0; k < 9; k++)
-            b[32 * k] = make_float4(U.e[k].re.v.x, U.e[k].re.v.y, U.e[k].im.v.x, U.e[k].im.v.y);
-    }
-    // one lattice site: lane 0 or 1 of the pair, widened to FP64
-    __device__ __forceinline__ M3<double> load_lane(int mu, int par, int s, int lane) const {
-        const float *b = reinterpret_cast<const float *>(p + base(mu, par, s));
-        M3<double> U;
-#pragma unroll
-        for (int k = 0; k < 9; k++) {
-            U.e[k].re = (double)b[128 * k + lane];
-            U.e[k].im = (double)b[128 * k + 2 + lane];
-        }
-        return U;
-    }
-    __device__ __forceinline__ void store_lane(int mu, int par, int s, int lane, const M3<double> &U) const {
-        float *b = reinterpret_cast<float *>(p + base(mu, par, s));
-#pragma unroll
-        for (int k = 0; k < 9; k++) {
-            b[128 * k + lane] = (float)U.e[k].re;
-            b[128 * k + 2 + lane] = (float)U.e[k].im;
-        }
+        for (int k = 0; k < 4; k++)
+            b[32 * k] = make_float4(U.e[2 * k].re, U.e[2 * k].im, U.e[2 * k + 1].re, U.e[2 * k + 1].im);
+        p2[at2(mu, par, s)] = make_float2(U.e[8].re, U.e[8].im);
     }
 };
 
-template <typename R> struct ForceField;
+template <typename T> struct ForceField;
 
 template <> struct ForceField<double> {
     double2 *p;
@@ -275,7 +212,7 @@ template <> struct ForceField<double> {
     __device__ __forceinline__ AH8<double> load(int mu, int par, int s) const {
         const double2 *b = p + base(mu, par, s);
         AH8<double> Z;
-        const double2 v0 = b[0], v1 = b[32], v2 = b[64], v3 = b[96];
+        double2 v0 = b[0], v1 = b[32], v2 = b[64], v3 = b[96];
         Z.a = v0.x; Z.d = v0.y;
         Z.b = cx(v1.x, v1.y); Z.c = cx(v2.x, v2.y); Z.e = cx(v3.x, v3.y);
         return Z;
@@ -289,28 +226,24 @@ template <> struct ForceField<double> {
     }
 };
 
-template <> struct ForceField<f32x2> {
+template <> struct ForceField<float> {
     float4 *p;
     int Vh, Vh32;
     GLAC_HD size_t base(int mu, int par, int s) const {
-        return (size_t)(mu * 2 + par) * 4 * (size_t)Vh32 + (size_t)(s >> 5) * 128 + (size_t)(s & 31);
+        return (size_t)(mu * 2 + par) * 2 * (size_t)Vh32 + (size_t)(s >> 5) * 64 + (size_t)(s & 31);
     }
-    __device__ __forceinline__ AH8<f32x2> load(int mu, int par, int s) const {
+    __device__ __forceinline__ AH8<float> load(int mu, int par, int s) const {
         const float4 *b = p + base(mu, par, s);
-        AH8<f32x2> Z;
-        const float4 v0 = b[0], v1 = b[32], v2 = b[64], v3 = b[96];
-        Z.a = f32x2(v0.x, v0.y); Z.d = f32x2(v0.z, v0.w);
-        Z.b = cx(f32x2(v1.x, v1.y), f32x2(v1.z, v1.w));
-        Z.c = cx(f32x2(v2.x, v2.y), f32x2(v2.z, v2.w));
-        Z.e = cx(f32x2(v3.x, v3.y), f32x2(v3.z, v3.w));
+        AH8<float> Z;
+        float4 v0 = b[0], v1 = b[32];
+        Z.a = v0.x; Z.d = v0.y; Z.b = cx(v0.z, v0.w);
+        Z.c = cx(v1.x, v1.y); Z.e = cx(v1.z, v1.w);
         return Z;
     }
-    __device__ __forceinline__ void store(int mu, int par, int s, const AH8<f32x2> &Z) const {
+    __device__ __forceinline__ void store(int mu, int par, int s, const AH8<float> &Z) const {
         float4 *b = p + base(mu, par, s);
-        b[0] = make_float4(Z.a.v.x, Z.a.v.y, Z.d.v.x, Z.d.v.y);
-        b[32] = make_float4(Z.b.re.v.x, Z.b.re.v.y, Z.b.im.v.x, Z.b.im.v.y);
-        b[64] = make_float4(Z.c.re.v.x, Z.c.re.v.y, Z.c.im.v.x, Z.c.im.v.y);
-        b[96] = make_float4(Z.e.re.v.x, Z.e.re.v.y, Z.e.im.v.x, Z.e.im.v.y);
+        b[0] = make_float4(Z.a, Z.d, Z.b.re, Z.b.im);
+        b[32] = make_float4(Z.c.re, Z.c.im, Z.e.re, Z.e.im);
     }
 };
 

@@ -2,9 +2,8 @@
 //
 // A matrix is 9 complex numbers, row-major, matching the reference element
 // order (i,j) -> re [6i+2j], im [6i+2j+1] (GLAC/math/matrices/su3.h:18-22).
-// The real type R is a template parameter: double (FP64 path), float (FP32
-// path) or f32x2 (two independent links per thread in packed FP32 lanes,
-// issued as sm_100 fma.rn.f32x2).
+// The real type R is a template parameter: double (FP64 path) or float (FP32
+// path).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -14,48 +13,10 @@
 
 namespace glac {
 
-// ---------------------------------------------------------------------------
-// Packed FP32 pair: lane x and lane y carry two independent computations.
-// ---------------------------------------------------------------------------
-struct f32x2 {
-    float2 v;
-    GLAC_HD f32x2() {}
-    GLAC_HD explicit f32x2(float s) { v.x = s; v.y = s; }
-    GLAC_HD f32x2(float a, float b) { v.x = a; v.y = b; }
-};
-
-#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000)
-#define GLAC_HAVE_F32X2 1
-#endif
-
-GLAC_HD f32x2 operator+(f32x2 a, f32x2 b) {
-#ifdef GLAC_HAVE_F32X2
-    f32x2 r; r.v = __fadd2_rn(a.v, b.v); return r;
-#else
-    return f32x2(a.v.x + b.v.x, a.v.y + b.v.y);
-#endif
-}
-GLAC_HD f32x2 operator-(f32x2 a, f32x2 b) { return f32x2(a.v.x - b.v.x, a.v.y - b.v.y); }
-GLAC_HD f32x2 operator-(f32x2 a) { return f32x2(-a.v.x, -a.v.y); }
-GLAC_HD f32x2 operator*(f32x2 a, f32x2 b) {
-#ifdef GLAC_HAVE_F32X2
-    f32x2 r; r.v = __fmul2_rn(a.v, b.v); return r;
-#else
-    return f32x2(a.v.x * b.v.x, a.v.y * b.v.y);
-#endif
-}
-GLAC_HD f32x2 fmaR(f32x2 a, f32x2 b, f32x2 c) {
-#ifdef GLAC_HAVE_F32X2
-    f32x2 r; r.v = __ffma2_rn(a.v, b.v, c.v); return r;
-#else
-    return f32x2(fmaf(a.v.x, b.v.x, c.v.x), fmaf(a.v.y, b.v.y, c.v.y));
-#endif
-}
 GLAC_HD double fmaR(double a, double b, double c) { return fma(a, b, c); }
 GLAC_HD float fmaR(float a, float b, float c) { return fmaf(a, b, c); }
 
 template <typename R> GLAC_HD R rzero() { return R(0); }
-template <> GLAC_HD f32x2 rzero<f32x2>() { return f32x2(0.f); }
 
 // ---------------------------------------------------------------------------
 // Complex numbers and 3x3 complex matrices
@@ -120,11 +81,6 @@ template <typename R> GLAC_HD void set_identity(M3<R> &a) {
     set_zero(a);
     a.e[0].re = R(1.f); a.e[4].re = R(1.f); a.e[8].re = R(1.f);
 }
-template <> GLAC_HD void set_identity<f32x2>(M3<f32x2> &a) {
-    set_zero(a);
-    a.e[0].re = f32x2(1.f); a.e[4].re = f32x2(1.f); a.e[8].re = f32x2(1.f);
-}
-
 // C = A B
 template <typename R> GLAC_HD M3<R> mul(const M3<R> &A, const M3<R> &B) {
     M3<R> C;

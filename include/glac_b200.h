@@ -44,7 +44,7 @@ typedef enum { GLAC_FP64 = 0, GLAC_FP32 = 1 } glac_precision;
 typedef enum { GLAC_EXP_MORNINGSTAR = 0, GLAC_EXP_LUSCHER = 1, GLAC_EXP_TAYLOR2 = 2, GLAC_EXP_TAYLOR4 = 3 } glac_exp;
 
 typedef struct {
-    int dims[4];            /* Nx, Ny, Nz, Nt; each even and >= 4, Nt % 4 == 0 for FP32 (NSpatial/NTemporal) */
+    int dims[4];            /* Nx, Ny, Nz, Nt; each even and >= 4 (NSpatial/NTemporal) */
     double beta;            /* "beta" */
     int precision;          /* glac_precision */
     int n_updates;          /* "NUpdates": Metropolis hits per link */
@@ -112,6 +112,17 @@ glac_status glac_flow_configuration(glac_ctx *ctx, const double *host_links, int
  * n_steps flow steps of the current field (CUDA events on the context's
  * stream); advances the field by n_steps. */
 glac_status glac_flow_stage_times(glac_ctx *ctx, int n_steps, double *seconds3);
+
+/* Launch-variant autotuner (no reference counterpart): times each launch
+ * variant (register cap / resident blocks per SM) of the flow-stage,
+ * Metropolis and observable kernels on this lattice, reps calls each, keeps the
+ * fastest, and restores the field and random stream.  report (may be NULL)
+ * receives 3 x 4 seconds-per-call entries [family][variant], 0 where unused. */
+glac_status glac_autotune(glac_ctx *ctx, int reps, double *report);
+/* The chosen variant per family (flow, metropolis, observables), and a setter
+ * for a previously tuned choice. */
+glac_status glac_get_tuning(glac_ctx *ctx, int *variants3);
+glac_status glac_set_tuning(glac_ctx *ctx, const int *variants3);
 
 /* ---- test exports (parity checks against the reference) ------------------ */
 /* Staples of every link of the current field, host layout (computeStaple). */

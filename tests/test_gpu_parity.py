@@ -133,10 +133,29 @@ def test_fp32_lanes_across_the_t_cut(g, oracle):
         assert rel_err(L.get_links(), want_flow) < 1e-5
 
 
-def test_fp32_needs_nt_multiple_of_four(g):
-    with pytest.raises(g.GlacError) as e:
-        g.Lattice((4, 4, 4, 6), precision="fp32")
-    assert e.value.status == g.GLAC_ERR_ARG
+def test_autotune_restores_state_and_keeps_results(g, oracle):
+    N = (8, 8, 8, 8)
+    start = oracle.haar_field(N, 21)
+    for prec in ("fp64", "fp32"):
+        with lattice(g, N, prec, seed=9) as A, lattice(g, N, prec, seed=9) as B:
+            A.set_links(start)
+            B.set_links(start)
+            rep = A.autotune(2)
+            assert np.array_equal(A.get_links(), start if prec == "fp64" else B.get_links())
+            for fam in ("flow", "metropolis", "observables"):
+                assert rep[fam][0] > 0
+            # every variant computes the same thing; the chain continues identically
+            acc_a, acc_b = A.metropolis(2), B.metropolis(2)
+            assert acc_a == acc_b
+            assert np.array_equal(A.get_links(), B.get_links())
+            for v in range(4):
+                try:
+                    A.tuning = [v, v, v]
+                except g.GlacError:
+                    continue
+                A.set_links(start)
+                B.set_links(start)
+                assert np.array_equal(A.flow(2), B.flow(2))
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
