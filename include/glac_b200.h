@@ -144,6 +144,28 @@ glac_status glac_accept_fed(int precision, double beta, long n_links, int n_hits
                             const double *host_A, const double *host_X, const double *host_r,
                             unsigned char *host_accept);
 
+/* ---- allocation-free measurement ------------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc --
+ * code under a host framework that owns all device memory through its own pool
+ * and forbids library allocations, latency-critical phases where a driver
+ * allocation would synchronise the device, deployments whose device memory is
+ * fixed at load time -- this entry point measures [plaq, topc, energy,
+ * topct[Nt]] of a field without allocating anything: dev_links is a device
+ * pointer to the field in the host layout above (FP64), dev_obs a device
+ * pointer to 3 + Nt doubles, stream a cudaStream_t (NULL: default stream); the
+ * call is asynchronous on that stream.  Its only working memory is a fixed
+ * 96 KiB device array inside this library (4096 partial-sum slots), held by
+ * every GPU that loads the library until the process exits; Nt above 4096 is
+ * rejected with GLAC_ERR_ARG.  The first call on a device resolves that array's
+ * address (cudaGetSymbolAddress), so make the first call on each device outside
+ * any stream capture.  All calls share the array and every call overwrites the
+ * slots it reads, so nothing needs clearing between calls -- but calls that
+ * overlap on the GPU (different streams, or different host threads, at the same
+ * time) race on it and must be serialised by the caller.  Errors:
+ * glac_noalloc_error(). */
+glac_status glac_measure_noalloc(const int dims[4], const double *dev_links, double *dev_obs, void *stream);
+const char *glac_noalloc_error(void);
+
 /* ---- gauge-field files (GLAC/io/fieldio.cpp) ----------------------------- */
 /* Read a GLAC .bin configuration (per site 4 links x 18 doubles, x fastest;
  * fieldio.cpp:195-257) or, with chroma != 0, its byte-swapped Chroma variant
