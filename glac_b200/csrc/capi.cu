@@ -263,6 +263,17 @@ glac_status glac_hot_start(glac_ctx *c, uint64_t seed) {
     });
 }
 
+glac_status glac_rst_start(glac_ctx *c, uint64_t seed) {
+    return guarded(c, [&] {
+        if (c->d.precision == GLAC_FP64) launch_rst_start(c->g, f64(c, c->cur), c->d.su3_eps, seed, c->d.stream_id, c->stream);
+        else launch_rst_start(c->g, f32(c, c->cur), c->d.su3_eps, seed, c->d.stream_id, c->stream);
+        ck_launch("rst start");
+        c->launches++;
+        c->has_field = true;
+        return GLAC_OK;
+    });
+}
+
 glac_status glac_set_links_device(glac_ctx *c, const double *dev) {
     return guarded(c, [&] {
         if (!dev) { c->err = "null field"; return GLAC_ERR_ARG; }
@@ -311,6 +322,23 @@ glac_status glac_get_links(glac_ctx *c, double *host) {
                            c->stream),
            "D2H links");
         ck(cudaStreamSynchronize(c->stream), "sync");
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_copy_field(glac_ctx *dst, glac_ctx *src) {
+    if (!dst || !src) return GLAC_ERR_ARG;
+    return guarded(dst, [&] {
+        if (!src->has_field) { dst->err = "source has no field"; return GLAC_ERR_STATE; }
+        if (src->d.precision != dst->d.precision || memcmp(src->d.dims, dst->d.dims, sizeof(src->d.dims))) {
+            dst->err = "contexts differ in precision or dimensions";
+            return GLAC_ERR_ARG;
+        }
+        ck(cudaStreamSynchronize(src->stream), "sync source");
+        ck(cudaMemcpyAsync(dst->field[dst->cur], src->field[src->cur], field_bytes(dst->d, dst->g),
+                           cudaMemcpyDeviceToDevice, dst->stream),
+           "copy field");
+        dst->has_field = true;
         return GLAC_OK;
     });
 }

@@ -549,6 +549,33 @@ __global__ void k_haar(Geom g, LinkField<T> L, uint32_t k0, uint32_t k1, uint32_
     L.store(mu, p, s, to_t<T>(Z));
 }
 
+// Random links near unity: each link is one RST proposal matrix (the
+// reference's RST hot start, GLAC/system.cpp:205-210 with generateRST,
+// su3matrixgenerator.h:170-196), drawn from the Philox stream with sweep
+// counter 0xFFFFFFFF.
+template <typename T>
+__global__ void k_rst_start(Geom g, LinkField<T> L, double eps, uint32_t k0, uint32_t k1, uint32_t stream_id) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+    const Site n = site_from_ps(g, p, s);
+    M3<double> X;
+    double r;
+    draw_proposal<double>(k0, k1, (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex, 0xFFFFFFFFu, stream_id, 0, eps,
+                          sqrt(1.0 - eps * eps), X, r);
+    L.store(mu, p, s, to_t<T>(X));
+}
+template <typename T>
+void launch_rst_start(const Geom &g, const LinkField<T> &L, double eps, uint64_t seed, uint32_t stream_id,
+                      cudaStream_t st) {
+    k_rst_start<T><<<dim3((g.Vh + 127) / 128, 8), 128, 0, st>>>(g, L, eps, (uint32_t)seed, (uint32_t)(seed >> 32),
+                                                                stream_id);
+}
+template void launch_rst_start<double>(const Geom &, const LinkField<double> &, double, uint64_t, uint32_t,
+                                       cudaStream_t);
+template void launch_rst_start<float>(const Geom &, const LinkField<float> &, double, uint64_t, uint32_t,
+                                      cudaStream_t);
+
 template <typename T>
 __global__ void k_cold(Geom g, LinkField<T> L) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;

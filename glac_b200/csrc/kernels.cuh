@@ -74,6 +74,9 @@ void launch_haar(const Geom &g, const LinkField<T> &L, uint64_t seed, uint32_t s
 template <typename T>
 void launch_cold(const Geom &g, const LinkField<T> &L, cudaStream_t st);
 template <typename T>
+void launch_rst_start(const Geom &g, const LinkField<T> &L, double eps, uint64_t seed, uint32_t stream_id,
+                      cudaStream_t st);
+template <typename T>
 void launch_reunitarize(const Geom &g, const LinkField<T> &L, cudaStream_t st);
 template <typename T>
 void launch_aos_to_soa(const Geom &g, const double *aos, const LinkField<T> &L, cudaStream_t st);

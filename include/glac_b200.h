@@ -79,12 +79,18 @@ glac_status glac_set_option(glac_ctx *ctx, const char *key, long value);
 glac_status glac_cold_start(glac_ctx *ctx);
 /* Seeded Haar-random start (replaces the hot start, GLAC/system.cpp:200-214). */
 glac_status glac_hot_start(glac_ctx *ctx, uint64_t seed);
+/* Every link a random RST matrix near unity with spread su3_eps (the
+ * reference's RSTHotStart, GLAC/system.cpp:205-210). */
+glac_status glac_rst_start(glac_ctx *ctx, uint64_t seed);
 /* Host <-> device in the reference layout; FP32 contexts convert. */
 glac_status glac_set_links(glac_ctx *ctx, const double *host_links);
 glac_status glac_get_links(glac_ctx *ctx, double *host_links);
 /* Same, from / to device memory in the host layout (no host copy). */
 glac_status glac_set_links_device(glac_ctx *ctx, const double *dev_links);
 glac_status glac_get_links_device(glac_ctx *ctx, double *dev_links);
+/* Device copy of src's field into dst (same dims and precision); the flow
+ * lattice copy of System::copyToFlowLattice (GLAC/system.cpp:179-188). */
+glac_status glac_copy_field(glac_ctx *dst, glac_ctx *src);
 /* FP64 Gram-Schmidt projection of every link back onto SU(3). */
 glac_status glac_reunitarize(glac_ctx *ctx);
 /* max over links and entries of |U U^+ - 1|. */
