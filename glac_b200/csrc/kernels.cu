@@ -20,11 +20,23 @@ namespace glac {
 // together cover one region of the lattice for all planes, so the neighbour
 // links they share are read from HBM once and then hit in L2.
 // ---------------------------------------------------------------------------
+// Site-block shapes (blocks of 128 threads):
+//   shape 0: a block = 128 consecutive sites of one plane, blocks of the 8
+//            planes interleaved;
+//   shape 1: a block = the same 16 sites in all 8 planes (half-warp per plane),
+//            so the neighbour links shared by the 8 link directions of a site
+//            are re-read from L1.
 template <typename T, int KIND, int STAGE>
 __device__ __forceinline__ void flow_stage_body(const Geom &g, const LinkField<T> &in, const LinkField<T> &out,
-                                                const ForceField<T> &zf, T alpha, T beta) {
-    const int plane = blockIdx.x & 7;
-    const int s = (blockIdx.x >> 3) * blockDim.x + threadIdx.x;
+                                                const ForceField<T> &zf, T alpha, T beta, int shape) {
+    int plane, s;
+    if (shape == 1) {
+        plane = threadIdx.x >> 4;
+        s = blockIdx.x * 16 + (threadIdx.x & 15);
+    } else {
+        plane = blockIdx.x & 7;
+        s = (blockIdx.x >> 3) * blockDim.x + threadIdx.x;
+    }
     if (s >= g.Vh) return;
     const int mu = plane >> 1, p = plane & 1;
     const Site n = site_from_ps(g, p, s);
@@ -48,8 +60,8 @@ __device__ __forceinline__ void flow_stage_body(const Geom &g, const LinkField<T
 #define GLAC_FLOW_KERNEL(NAME, ATTR)                                                                      \
     template <typename T, int KIND, int STAGE>                                                           \
     __global__ void ATTR NAME(Geom g, LinkField<T> in, LinkField<T> out,                                 \
-                                                     ForceField<T> zf, T alpha, T beta) {                \
-        flow_stage_body<T, KIND, STAGE>(g, in, out, zf, alpha, beta);                                    \
+                                                     ForceField<T> zf, T alpha, T beta, int shape) {     \
+        flow_stage_body<T, KIND, STAGE>(g, in, out, zf, alpha, beta, shape);                             \
     }
 GLAC_FLOW_KERNEL(k_flow_stage, __launch_bounds__(128))
 GLAC_FLOW_KERNEL(k_flow_stage_r128, __maxnreg__(128))
@@ -60,8 +72,10 @@ GLAC_FLOW_KERNEL(k_flow_stage_r72, __maxnreg__(72))
 
 // Launch-bound variants (minimum resident blocks of 128 threads per SM, i.e.
 // the register cap) that the autotuner chooses among; variant 0 is the default.
-// Register caps per variant ([fp64, fp32]; 0 = no cap, -1 = unused slot).
-const int kFlowRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 80, 72, 96}};
+// Register caps per variant ([fp64, fp32]; 0 = no cap, -1 = unused slot); the
+// flow family also varies the site-block shape.
+const int kFlowRegs[2][kMaxVariants] = {{0, 128, 0, -1}, {0, 80, 0, 80}};
+const int kFlowShape[2][kMaxVariants] = {{0, 0, 1, 0}, {0, 0, 1, 1}};
 const int kMetroRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 96, 80, 128}};
 const int kObsRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 128, -1, -1}};
 
@@ -76,15 +90,20 @@ int variant_regs(Family f, bool fp32, int v) {
     return (v >= 0 && v < kMaxVariants) ? t[fp32 ? 1 : 0][v] : 0;
 }
 
+int variant_shape(Family f, bool fp32, int v) {
+    return (f == FAM_FLOW && v >= 0 && v < kMaxVariants) ? kFlowShape[fp32 ? 1 : 0][v] : 0;
+}
+
 template <typename T, int KIND, int STAGE>
-static void flow_dispatch(int regs, dim3 grid, cudaStream_t st, const Geom &g, const LinkField<T> &in,
+static void flow_dispatch(int regs, int shape, cudaStream_t st, const Geom &g, const LinkField<T> &in,
                           const LinkField<T> &out, const ForceField<T> &zf, T a, T b) {
+    const dim3 grid = shape == 1 ? dim3((g.Vh + 15) / 16) : dim3(8 * ((g.Vh + 127) / 128));
     switch (regs) {
-    case 128: k_flow_stage_r128<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
-    case 96: k_flow_stage_r96<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
-    case 80: k_flow_stage_r80<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
-    case 72: k_flow_stage_r72<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
-    default: k_flow_stage<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
+    case 128: k_flow_stage_r128<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, shape); break;
+    case 96: k_flow_stage_r96<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, shape); break;
+    case 80: k_flow_stage_r80<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, shape); break;
+    case 72: k_flow_stage_r72<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, shape); break;
+    default: k_flow_stage<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, shape); break;
     }
 }
 
@@ -95,14 +114,14 @@ void launch_flow_stage(const Geom &g, const LinkField<T> &in, const LinkField<T>
     const T a = (T)alpha, b = (T)beta;
     const bool fp32 = sizeof(T) == 4;
     if (kind == EXP_MORNINGSTAR) {
-        const int regs = variant_regs(FAM_FLOW, fp32, variant);
-        if (stage == 0) flow_dispatch<T, 0, 0>(regs, grid, st, g, in, out, zf, a, b);
-        else if (stage == 1) flow_dispatch<T, 0, 1>(regs, grid, st, g, in, out, zf, a, b);
-        else flow_dispatch<T, 0, 2>(regs, grid, st, g, in, out, zf, a, b);
+        const int regs = variant_regs(FAM_FLOW, fp32, variant), shape = variant_shape(FAM_FLOW, fp32, variant);
+        if (stage == 0) flow_dispatch<T, 0, 0>(regs, shape, st, g, in, out, zf, a, b);
+        else if (stage == 1) flow_dispatch<T, 0, 1>(regs, shape, st, g, in, out, zf, a, b);
+        else flow_dispatch<T, 0, 2>(regs, shape, st, g, in, out, zf, a, b);
         return;
     }
 #define GLAC_FLOW_CASE(K, S) \
-    if (kind == K && stage == S) { k_flow_stage<T, K, S><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); return; }
+    if (kind == K && stage == S) { k_flow_stage<T, K, S><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, 0); return; }
     GLAC_FLOW_CASE(1, 0) GLAC_FLOW_CASE(1, 1) GLAC_FLOW_CASE(1, 2)
     GLAC_FLOW_CASE(2, 0) GLAC_FLOW_CASE(2, 1) GLAC_FLOW_CASE(2, 2)
     GLAC_FLOW_CASE(3, 0) GLAC_FLOW_CASE(3, 1) GLAC_FLOW_CASE(3, 2)

@@ -57,7 +57,8 @@ ObsPlan make_obs_plan(const Geom &g);
 enum Family { FAM_FLOW = 0, FAM_METRO = 1, FAM_OBS = 2 };
 constexpr int kMaxVariants = 4;
 int num_variants(Family f, bool fp32);
-int variant_regs(Family f, bool fp32, int v);  // register cap of a variant (0 = none)
+int variant_regs(Family f, bool fp32, int v);   // register cap of a variant (0 = none)
+int variant_shape(Family f, bool fp32, int v);  // flow site-block shape of a variant (0 = one plane per block)
 
 template <typename T>
 void launch_flow_stage(const Geom &g, const LinkField<T> &in, const LinkField<T> &out, const ForceField<T> &zf,
