@@ -130,14 +130,15 @@ template <> struct SeriesTerms<double> { static const int n = 16; };
 
 // exp(iQ) = sum_n i^n Q^n / n!,  Q^n = a_n 1 + b_n Q + g_n Q^2 with
 // a_{n+1} = c0 g_n, b_{n+1} = a_n + c1 g_n, g_{n+1} = b_n  (a, b, g carry 1/n!).
-template <typename R> GLAC_HD void ms_series(R c0, R c1, Cx<R> &f0, Cx<R> &f1, Cx<R> &f2) {
+// With M1 set, f0 omits the n = 0 term: the coefficients of exp(iQ) - 1.
+template <typename R, bool M1 = false> GLAC_HD void ms_series(R c0, R c1, Cx<R> &f0, Cx<R> &f1, Cx<R> &f2) {
     R a = R(1.f), b = rzero<R>(), gg = rzero<R>();
     R z = rzero<R>();
     f0 = cx(z, z); f1 = cx(z, z); f2 = cx(z, z);
 #pragma unroll
     for (int n = 0; n < SeriesTerms<R>::n; n++) {
         switch (n & 3) {
-        case 0: f0.re = f0.re + a; f1.re = f1.re + b; f2.re = f2.re + gg; break;
+        case 0: if (!M1 || n > 0) f0.re = f0.re + a; f1.re = f1.re + b; f2.re = f2.re + gg; break;
         case 1: f0.im = f0.im + a; f1.im = f1.im + b; f2.im = f2.im + gg; break;
         case 2: f0.re = f0.re - a; f1.re = f1.re - b; f2.re = f2.re - gg; break;
         default: f0.im = f0.im - a; f1.im = f1.im - b; f2.im = f2.im - gg; break;
@@ -150,7 +151,8 @@ template <typename R> GLAC_HD void ms_series(R c0, R c1, Cx<R> &f0, Cx<R> &f1, C
         b = b1;
     }
 }
-template <> GLAC_HD void ms_series<double>(double c0, double c1, Cx<double> &f0, Cx<double> &f1, Cx<double> &f2) {
+template <> GLAC_HD void ms_series<double, false>(double c0, double c1, Cx<double> &f0, Cx<double> &f1,
+                                                   Cx<double> &f2) {
     double a = 1.0, b = 0.0, gg = 0.0;
     f0 = cx(0.0, 0.0); f1 = cx(0.0, 0.0); f2 = cx(0.0, 0.0);
 #pragma unroll
@@ -192,17 +194,20 @@ GLAC_HD M3<R> ms_combine(const HQ<R> &Q, const HQ2<R> &S, Cx<R> f0, Cx<R> f1, Cx
     return E;
 }
 
-template <typename R> GLAC_HD M3<R> expm_morningstar(const AH8<R> &Z) {
+// exp(Z), or with M1 set exp(Z) - 1: the flow's link update U' = U + (exp(Z) - 1) U
+// rounds once at the magnitude of U instead of carrying exp(Z)'s rounding at
+// ulp(1), which in FP32 is most of a small flow increment's precision.
+template <typename R, bool M1 = false> GLAC_HD M3<R> expm_morningstar(const AH8<R> &Z) {
     const HQ<R> Q = herm_from_ah(Z);
     const HQ2<R> S = herm_square(Q);
     R c0, c1;
     invariants(Q, S, c0, c1);
     Cx<R> f0, f1, f2;
     if (c1 < R(GLAC_SERIES_C1_MAX)) {
-        ms_series(c0, c1, f0, f1, f2);
+        ms_series<R, M1>(c0, c1, f0, f1, f2);
     } else {
         const ExpCoef f = ms_coefficients((double)c0, (double)c1);
-        f0 = cx(from_d<R>(f.f0r), from_d<R>(f.f0i));
+        f0 = cx(from_d<R>(M1 ? f.f0r - 1.0 : f.f0r), from_d<R>(f.f0i));
         f1 = cx(from_d<R>(f.f1r), from_d<R>(f.f1i));
         f2 = cx(from_d<R>(f.f2r), from_d<R>(f.f2i));
     }
@@ -278,7 +283,7 @@ template <typename R> GLAC_HD M3<R> expm_taylor(const M3<R> &Q, int deg) {
 }
 
 template <typename R> GLAC_HD M3<R> expm(int kind, const AH8<R> &Z) {
-    if (kind == EXP_MORNINGSTAR) return expm_morningstar(Z);
+    if (kind == EXP_MORNINGSTAR) return expm_morningstar<R>(Z);
     M3<R> M = ah_to_m3(Z);
     if (kind == EXP_LUSCHER) return expm_luscher(M);
     return expm_taylor(M, kind == EXP_TAYLOR2 ? 2 : 4);

@@ -26,17 +26,11 @@ namespace glac {
 //   shape 1: a block = the same 16 sites in all 8 planes (half-warp per plane),
 //            so the neighbour links shared by the 8 link directions of a site
 //            are re-read from L1.
-template <typename T, int KIND, int STAGE>
+template <typename T, int KIND, int STAGE, int SHAPE>
 __device__ __forceinline__ void flow_stage_body(const Geom &g, const LinkField<T> &in, const LinkField<T> &out,
-                                                const ForceField<T> &zf, T alpha, T beta, int shape) {
-    int plane, s;
-    if (shape == 1) {
-        plane = threadIdx.x >> 4;
-        s = blockIdx.x * 16 + (threadIdx.x & 15);
-    } else {
-        plane = blockIdx.x & 7;
-        s = (blockIdx.x >> 3) * blockDim.x + threadIdx.x;
-    }
+                                                const ForceField<T> &zf, T alpha, T beta) {
+    const int plane = SHAPE == 1 ? int(threadIdx.x >> 4) : int(blockIdx.x & 7);
+    const int s = SHAPE == 1 ? int(blockIdx.x * 16 + (threadIdx.x & 15)) : int((blockIdx.x >> 3) * 128 + threadIdx.x);
     if (s >= g.Vh) return;
     const int mu = plane >> 1, p = plane & 1;
     const Site n = site_from_ps(g, p, s);
@@ -52,30 +46,33 @@ __device__ __forceinline__ void flow_stage_body(const Geom &g, const LinkField<T
         M = ah_axpby(alpha, Z, beta, W);
         if (STAGE == 1) zf.store(mu, p, s, M);
     }
-    out.store(mu, p, s, mul(expm<T>(KIND, M), U));
+    if (KIND == EXP_MORNINGSTAR) {
+        // U' = U + (exp(M) - 1) U: the small product first, one rounding at |U|
+        out.store(mu, p, s, mul_plus_right(expm_morningstar<T, true>(M), U));
+    } else {
+        out.store(mu, p, s, mul(expm<T>(KIND, M), U));
+    }
 }
 
-// One __global__ per register cap (REGS = 0: the compiler's own choice); the
-// autotuner picks among them per lattice.
+// One __global__ per register cap (none: the compiler's own choice under
+// 128-thread launch bounds) and site-block shape; the autotuner picks among
+// them per lattice.
 #define GLAC_FLOW_KERNEL(NAME, ATTR)                                                                      \
-    template <typename T, int KIND, int STAGE>                                                           \
-    __global__ void ATTR NAME(Geom g, LinkField<T> in, LinkField<T> out,                                 \
-                                                     ForceField<T> zf, T alpha, T beta, int shape) {     \
-        flow_stage_body<T, KIND, STAGE>(g, in, out, zf, alpha, beta, shape);                             \
+    template <typename T, int KIND, int STAGE, int SHAPE>                                                \
+    __global__ void ATTR NAME(Geom g, LinkField<T> in, LinkField<T> out, ForceField<T> zf, T alpha,      \
+                              T beta) {                                                                  \
+        flow_stage_body<T, KIND, STAGE, SHAPE>(g, in, out, zf, alpha, beta);                             \
     }
 GLAC_FLOW_KERNEL(k_flow_stage, __launch_bounds__(128))
 GLAC_FLOW_KERNEL(k_flow_stage_r128, __maxnreg__(128))
-GLAC_FLOW_KERNEL(k_flow_stage_r96, __maxnreg__(96))
 GLAC_FLOW_KERNEL(k_flow_stage_r80, __maxnreg__(80))
-GLAC_FLOW_KERNEL(k_flow_stage_r72, __maxnreg__(72))
-#undef GLAC_FLOW_KERNEL
 
 // Launch-bound variants (minimum resident blocks of 128 threads per SM, i.e.
 // the register cap) that the autotuner chooses among; variant 0 is the default.
 // Register caps per variant ([fp64, fp32]; 0 = no cap, -1 = unused slot); the
 // flow family also varies the site-block shape.
-const int kFlowRegs[2][kMaxVariants] = {{0, 128, 0, -1}, {0, 80, 0, 80}};
-const int kFlowShape[2][kMaxVariants] = {{0, 0, 1, 0}, {0, 0, 1, 1}};
+const int kFlowRegs[2][kMaxVariants] = {{0, 128, 0, -1}, {0, 80, 0, -1}};
+const int kFlowShape[2][kMaxVariants] = {{0, 0, 1, 0}, {0, 0, 1, 0}};
 const int kMetroRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 96, 80, 128}};
 const int kObsRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 128, -1, -1}};
 
@@ -97,13 +94,21 @@ int variant_shape(Family f, bool fp32, int v) {
 template <typename T, int KIND, int STAGE>
 static void flow_dispatch(int regs, int shape, cudaStream_t st, const Geom &g, const LinkField<T> &in,
                           const LinkField<T> &out, const ForceField<T> &zf, T a, T b) {
-    const dim3 grid = shape == 1 ? dim3((g.Vh + 15) / 16) : dim3(8 * ((g.Vh + 127) / 128));
+    if (shape == 1) {
+        const dim3 grid((g.Vh + 15) / 16);
+        k_flow_stage<T, KIND, STAGE, 1><<<grid, 128, 0, st>>>(g, in, out, zf, a, b);
+        return;
+    }
+    const dim3 grid(8 * ((g.Vh + 127) / 128));
     switch (regs) {
-    case 128: k_flow_stage_r128<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, shape); break;
-    case 96: k_flow_stage_r96<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, shape); break;
-    case 80: k_flow_stage_r80<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, shape); break;
-    case 72: k_flow_stage_r72<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, shape); break;
-    default: k_flow_stage<T, KIND, STAGE><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, shape); break;
+    case 128: k_flow_stage_r128<T, KIND, STAGE, 0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
+    case 80:
+        if constexpr (sizeof(T) == 4) {
+            k_flow_stage_r80<T, KIND, STAGE, 0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b);
+            break;
+        }
+        [[fallthrough]];  // no 80-register FP64 variant
+    default: k_flow_stage<T, KIND, STAGE, 0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
     }
 }
 
@@ -121,7 +126,7 @@ void launch_flow_stage(const Geom &g, const LinkField<T> &in, const LinkField<T>
         return;
     }
 #define GLAC_FLOW_CASE(K, S) \
-    if (kind == K && stage == S) { k_flow_stage<T, K, S><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, 0); return; }
+    if (kind == K && stage == S) { k_flow_stage<T, K, S, 0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); return; }
     GLAC_FLOW_CASE(1, 0) GLAC_FLOW_CASE(1, 1) GLAC_FLOW_CASE(1, 2)
     GLAC_FLOW_CASE(2, 0) GLAC_FLOW_CASE(2, 1) GLAC_FLOW_CASE(2, 2)
     GLAC_FLOW_CASE(3, 0) GLAC_FLOW_CASE(3, 1) GLAC_FLOW_CASE(3, 2)

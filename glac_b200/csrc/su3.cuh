@@ -154,6 +154,23 @@ template <typename R> GLAC_HD void acc_mul_nd(M3<R> &Acc, const M3<R> &A, const 
         }
 }
 // Acc += A B
+// D U + U with each element's small sum D(i,:) U(:,j) formed first and U(i,j)
+// added last (one rounding at the magnitude of U); column by column, so a
+// column of U is dead once its three outputs are done.
+template <typename R> GLAC_HD M3<R> mul_plus_right(const M3<R> &D, const M3<R> &U) {
+    M3<R> V;
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            Cx<R> t = D(i, 0) * U(0, j);
+            t = cmac(t, D(i, 1), U(1, j));
+            t = cmac(t, D(i, 2), U(2, j));
+            V(i, j) = t + U(i, j);
+        }
+    return V;
+}
+
 template <typename R> GLAC_HD void acc_mul(M3<R> &Acc, const M3<R> &A, const M3<R> &B) {
 #pragma unroll
     for (int i = 0; i < 3; i++)

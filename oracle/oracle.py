@@ -202,6 +202,8 @@ class Reference:
         lib.ref_time_flow.restype = C.c_double
         lib.ref_time_flow_measure.argtypes = [_dp, C.c_int]
         lib.ref_time_flow_measure.restype = C.c_double
+        lib.ref_metropolis_chain.argtypes = [_dp, C.c_int, _dp]
+        lib.ref_metropolis_chain.restype = C.c_double
         lib.ref_time_metropolis.argtypes = [_dp, C.c_int, C.POINTER(C.c_double)]
         lib.ref_time_metropolis.restype = C.c_double
         lib.ref_time_observables.argtypes = [_dp, C.c_int]
@@ -274,6 +276,13 @@ class Reference:
         out = np.array(links, np.float64, copy=True, order="C")
         acc = self.lib.ref_metropolis(out, int(nsweeps))
         return out, acc
+
+    def metropolis_chain(self, links, nsweeps):
+        """nsweeps sweeps of one System: (links after, plaquette per sweep, acceptance)."""
+        out = np.array(links, np.float64, copy=True, order="C")
+        plaq = np.zeros(int(nsweeps))
+        acc = self.lib.ref_metropolis_chain(out, int(nsweeps), plaq)
+        return out, plaq, acc
 
     def metropolis_trace(self, links):
         nl, nh = 4 * self.V, self.nupdates

@@ -276,6 +276,28 @@ double ref_metropolis(double *links, int nsweeps) {
     return sys.m_acceptanceScore / double(nsweeps > 0 ? nsweeps : 1);
 }
 
+/* A Markov chain of nsweeps System::update sweeps from one System (so its
+ * generators run on, as in System::runMetropolis, GLAC/system.cpp:363-469),
+ * with the plaquette (GLAC/observables/plaquette.cpp:26-40) after every sweep
+ * in plaq[nsweeps].  Returns the mean acceptance per sweep. */
+double ref_metropolis_chain(double *links, int nsweeps, double *plaq) {
+    System sys;
+    setup_system(sys);
+    for (int mu = 0; mu < 4; mu++)
+        for (unsigned long s = 0; s < g_V; s++)
+            std::memcpy(sys.m_lattice[mu].m_sites[s].mat, links + (mu * g_V + s) * 18, 18 * sizeof(double));
+    Plaquette P(true);
+    for (int i = 0; i < nsweeps; i++) {
+        sys.update();
+        P.calculate(sys.m_lattice, 0);
+        plaq[i] = (*P.m_observable)[0];
+    }
+    for (int mu = 0; mu < 4; mu++)
+        for (unsigned long s = 0; s < g_V; s++)
+            std::memcpy(links + (mu * g_V + s) * 18, sys.m_lattice[mu].m_sites[s].mat, 18 * sizeof(double));
+    return sys.m_acceptanceScore / double(nsweeps > 0 ? nsweeps : 1);
+}
+
 /* One Metropolis sweep in System::update's order (x, y, z, t outer to inner, then
  * mu; GLAC/system.cpp:338-357) with the draws recorded: for each visited link in
  * visiting order, the link before its hits, its staple, the NUpdates proposals X
