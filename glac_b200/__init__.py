@@ -28,6 +28,9 @@ EXP_FUNCS = {"morningstar": 0, "luscher": 1, "taylor2": 2, "taylor4": 3}
 PRECISIONS = {"fp64": FP64, "fp32": FP32, "double": FP64, "float": FP32}
 
 
+MLP_NPARAMS = 1377  # GLAC_MLP_NPARAMS
+
+
 class GlacError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"glac status {status}: {message}")
@@ -109,6 +112,24 @@ def lib() -> C.CDLL:
     L.glac_accept_fed.argtypes = [C.c_int, C.c_double, C.c_long, C.c_int, _dp, _dp, _dp, _dp, _u8]
     L.glac_read_field.argtypes = [C.c_char_p, C.c_int * 4, C.c_int, _dp]
     L.glac_write_field.argtypes = [C.c_char_p, C.c_int * 4, _dp]
+    # learned proposal spread
+    L.glac_copy_field.argtypes = [P, P]
+    L.glac_set_proposal_net.argtypes = [P, C.c_void_p, C.c_double, C.c_double]
+    L.glac_esj_data.argtypes = [P, C.c_int, _dp, C.c_int, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_longlong, C.POINTER(C.c_longlong)]
+    L.glac_mlp_create.argtypes = [C.c_int, C.POINTER(P)]
+    L.glac_mlp_destroy.argtypes = [P]
+    L.glac_mlp_destroy.restype = None
+    L.glac_mlp_last_error.argtypes = [P]
+    L.glac_mlp_last_error.restype = C.c_char_p
+    L.glac_mlp_set_params.argtypes = [P, C.c_void_p]
+    L.glac_mlp_get_params.argtypes = [P, C.c_void_p]
+    L.glac_mlp_init.argtypes = [P, C.c_uint64, C.c_double, C.c_double, C.c_double]
+    L.glac_mlp_forward.argtypes = [P, C.c_void_p, C.c_longlong, C.c_double, C.c_double, C.c_void_p]
+    L.glac_mlp_loss_grad.argtypes = [P, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, _dp,
+                                     C.POINTER(C.c_double), C.c_void_p]
+    L.glac_mlp_train.argtypes = [P, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, _dp, C.c_int, C.c_longlong,
+                                 C.c_double, C.c_void_p]
     _lib = L
     return L
 
@@ -285,6 +306,31 @@ class Lattice:
         out = np.empty((4, self.V, 18), np.float64)
         self._ck(lib().glac_staples(self._ctx, out))
         return out
+
+    def set_proposal_net(self, params=None, eps_min=0.0, eps_max=1.0):
+        """Learned proposal spread from now on (params: GLAC_MLP_NPARAMS floats), or None for su3_eps."""
+        if params is None:
+            self._ck(lib().glac_set_proposal_net(self._ctx, None, 0.0, 0.0))
+            return
+        p = np.ascontiguousarray(params, np.float32)
+        if p.size != MLP_NPARAMS:
+            raise ValueError(f"need {MLP_NPARAMS} parameters")
+        self._ck(lib().glac_set_proposal_net(self._ctx, p.ctypes.data, float(eps_min), float(eps_max)))
+
+    def esj_data_ptr(self, eps_grid, trials, stride, snapshot, feat_ptr, esj_ptr, ids_ptr, capacity) -> int:
+        """Expected-squared-jump rows into device buffers (pointers); returns the row count."""
+        g = np.ascontiguousarray(eps_grid, np.float64)
+        n = C.c_longlong(0)
+        self._ck(lib().glac_esj_data(self._ctx, g.size, g, int(trials), int(stride), int(snapshot), feat_ptr,
+                                     esj_ptr if g.size else None, ids_ptr, int(capacity), C.byref(n)))
+        return n.value
+
+    def copy_from(self, other: "Lattice"):
+        """Device copy of another context's field (same dimensions and precision)."""
+        self._ck(lib().glac_copy_field(self._ctx, other._ctx))
+
+    def esj_rows(self, stride) -> int:
+        return 8 * ((self.V // 2) // int(stride))
 
     def force(self):
         out = np.empty((4, self.V, 18), np.float64)

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <exception>
@@ -30,6 +31,10 @@ struct glac_ctx {
     uint32_t sweep = 0;
     uint64_t launches = 0;
     int tune[3] = {0, 0, 0};  // chosen launch variant per kernel family (flow, metropolis, observables)
+    float *net_params = nullptr;  // learned proposal spread: FP32 parameters and their packed fragments
+    uint32_t *net_pack = nullptr;
+    float *esj_grid = nullptr;    // 64 floats
+    Proposal prop;                // prop.net null: the fixed spread su3_eps
     bool has_field = false;
     std::string err;
 };
@@ -223,6 +228,9 @@ void glac_destroy(glac_ctx *c) {
     if (c->acc_dev) cudaFree(c->acc_dev);
     if (c->staging) cudaFree(c->staging);
     if (c->scalar_dev) cudaFree(c->scalar_dev);
+    if (c->net_params) cudaFree(c->net_params);
+    if (c->net_pack) cudaFree(c->net_pack);
+    if (c->esj_grid) cudaFree(c->esj_grid);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -236,7 +244,14 @@ glac_status glac_sync(glac_ctx *c) {
 
 glac_status glac_set_option(glac_ctx *c, const char *key, long value) {
     if (!c || !key) return GLAC_ERR_ARG;
-    (void)value;
+    if (std::string(key) == "su2_sign_flips") {
+        if (value != 0 && value != 1) {
+            c->err = "su2_sign_flips takes 0 or 1";
+            return GLAC_ERR_ARG;
+        }
+        c->prop.flips = value != 0;
+        return GLAC_OK;
+    }
     c->err = std::string("unknown option ") + key;
     return GLAC_ERR_ARG;
 }
@@ -378,11 +393,11 @@ glac_status glac_metropolis(glac_ctx *c, int n_sweeps, double *acceptance) {
                 if (c->d.precision == GLAC_FP64)
                     launch_metropolis(c->g, f64(c, c->cur), mu, p, c->d.beta, c->d.su3_eps, c->d.n_updates,
                                       c->d.seed, c->sweep, c->d.stream_id, c->acc_dev, c->tune[FAM_METRO],
-                                      c->stream);
+                                      c->prop, c->stream);
                 else
                     launch_metropolis(c->g, f32(c, c->cur), mu, p, c->d.beta, c->d.su3_eps, c->d.n_updates,
                                       c->d.seed, c->sweep, c->d.stream_id, c->acc_dev, c->tune[FAM_METRO],
-                                      c->stream);
+                                      c->prop, c->stream);
                 ck_launch("metropolis");
                 c->launches++;
             }
@@ -508,11 +523,11 @@ glac_status glac_autotune(glac_ctx *c, int reps, double *report) {
                                 if (fp32)
                                     launch_metropolis(c->g, f32(c, c->cur), k >> 1, k & 1, c->d.beta, c->d.su3_eps,
                                                       c->d.n_updates, c->d.seed, c->sweep, c->d.stream_id, c->acc_dev,
-                                                      v, c->stream);
+                                                      v, c->prop, c->stream);
                                 else
                                     launch_metropolis(c->g, f64(c, c->cur), k >> 1, k & 1, c->d.beta, c->d.su3_eps,
                                                       c->d.n_updates, c->d.seed, c->sweep, c->d.stream_id, c->acc_dev,
-                                                      v, c->stream);
+                                                      v, c->prop, c->stream);
                                 ck_launch("metropolis");
                             }
                         } else measure_into(c, c->obs_dev);
@@ -692,6 +707,86 @@ glac_status glac_accept_fed(int precision, double beta, long n_links, int n_hits
         ck_launch("accept fed");
         ck(cudaMemcpy(host_U, U.p, mb, cudaMemcpyDeviceToHost), "D2H");
         if (ab) ck(cudaMemcpy(host_accept, acc.p, ab, cudaMemcpyDeviceToHost), "D2H");
+        return GLAC_OK;
+    });
+}
+
+
+glac_status glac_set_proposal_net(glac_ctx *c, const float *params, double eps_min, double eps_max) {
+    return guarded(c, [&] {
+        if (!params) {
+            c->prop.net = nullptr;
+            return GLAC_OK;
+        }
+        if (!(eps_min > 0.0 && eps_min < eps_max && eps_max <= 1.0)) {
+            c->err = "proposal spread range must satisfy 0 < eps_min < eps_max <= 1";
+            return GLAC_ERR_ARG;
+        }
+        for (int k = 0; k < kMlpParams; k++)
+            if (!std::isfinite(params[k])) {
+                c->err = "non-finite network parameter";
+                return GLAC_ERR_NONFINITE;
+            }
+        if (!c->net_params) ck(cudaMalloc(&c->net_params, kMlpParams * sizeof(float)), "alloc net");
+        if (!c->net_pack) ck(cudaMalloc(&c->net_pack, kPackWords * sizeof(uint32_t)), "alloc net");
+        ck(cudaMemcpyAsync(c->net_params, params, kMlpParams * sizeof(float), cudaMemcpyHostToDevice, c->stream),
+           "upload net");
+        launch_mlp_pack(c->net_params, c->net_pack, c->stream);
+        ck_launch("pack net");
+        c->launches++;
+        ck(cudaStreamSynchronize(c->stream), "sync");
+        c->prop.net = c->net_pack;
+        c->prop.eps_min = (float)eps_min;
+        c->prop.eps_max = (float)eps_max;
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_esj_data(glac_ctx *c, int n_eps, const double *eps_grid, int trials, int stride, uint32_t snapshot,
+                          float *dev_features, float *dev_esj, uint32_t *dev_link_ids, long long capacity,
+                          long long *n_rows) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        if (n_eps < 0 || n_eps > 64 || (n_eps > 0 && (!eps_grid || !dev_esj || trials < 1)) || !dev_features ||
+            stride < 1 || stride > c->g.Vh) {
+            c->err = "esj: need 0 <= n_eps <= 64 (grid, output and trials >= 1 when > 0), features, 1 <= stride <= V/2";
+            return GLAC_ERR_ARG;
+        }
+        if (c->d.n_updates > 16) {
+            c->err = "esj: at most 16 hits per link";
+            return GLAC_ERR_ARG;
+        }
+        for (int k = 0; k < n_eps; k++)
+            if (!(eps_grid[k] > 0.0 && eps_grid[k] <= 1.0)) {
+                c->err = "esj: spreads must lie in (0, 1]";
+                return GLAC_ERR_ARG;
+            }
+        const int ns = c->g.Vh / stride;
+        const int offset = (int)((snapshot * 7919u) % (uint32_t)stride);
+        const long long rows = 8ll * ns;
+        if (n_rows) *n_rows = rows;
+        if (rows > capacity) {
+            c->err = "esj: capacity below 8 * (V/2 / stride) rows";
+            return GLAC_ERR_ARG;
+        }
+        if (n_eps > 0) {
+            if (!c->esj_grid) ck(cudaMalloc(&c->esj_grid, 64 * sizeof(float)), "alloc grid");
+            float g32[64];
+            for (int k = 0; k < n_eps; k++) g32[k] = (float)eps_grid[k];
+            ck(cudaMemcpyAsync(c->esj_grid, g32, n_eps * sizeof(float), cudaMemcpyHostToDevice, c->stream), "grid");
+        }
+        if (c->d.precision == GLAC_FP64)
+            launch_esj(c->g, f64(c, c->cur), c->d.beta, c->d.n_updates, n_eps, c->esj_grid, trials, stride, offset, ns,
+                       c->d.seed, snapshot, c->d.stream_id, c->prop.flips, dev_features, dev_esj, dev_link_ids,
+                       c->stream);
+        else
+            launch_esj(c->g, f32(c, c->cur), c->d.beta, c->d.n_updates, n_eps, c->esj_grid, trials, stride, offset, ns,
+                       c->d.seed, snapshot, c->d.stream_id, c->prop.flips, dev_features, dev_esj, dev_link_ids,
+                       c->stream);
+        ck_launch("esj");
+        c->launches++;
+        ck(cudaStreamSynchronize(c->stream), "sync");
         return GLAC_OK;
     });
 }

@@ -2,6 +2,7 @@
 // fused clover observables with deterministic FP64 reductions, plus field
 // initialisation, reunitarisation and layout conversion.
 #include "kernels.cuh"
+#include "learned.cuh"
 
 #include <algorithm>
 #include <stdexcept>
@@ -160,10 +161,10 @@ template <> __device__ __forceinline__ float su_scalar<float>(double v) { return
 GLAC_HD double u_sym16(uint32_t h) { return ((double)h + 0.5) * (1.0 / 65536.0) - 0.5; }
 
 template <typename T>
-__device__ __forceinline__ void su2_near_unity(T u0, T u1, T u2, T u3, T eps, T sq1me, T out[4]) {
+__device__ __forceinline__ void su2_near_unity(T u0, T u1, T u2, T u3, T eps, T sq1me, bool flips, T out[4]) {
     // x0 = sign(u0) sqrt(1 - eps^2), x = eps u / |u|, normalised
-    // (GLAC/math/matrices/su3matrixgenerator.h:202-243)
-    T x0 = u0 < T(0) ? -sq1me : sq1me;
+    // (GLAC/math/matrices/su3matrixgenerator.h:202-243); without flips x0 > 0
+    T x0 = (flips && u0 < T(0)) ? -sq1me : sq1me;
     T rn = sqrt(u1 * u1 + u2 * u2 + u3 * u3) / eps;
     T x1 = u1 / rn, x2 = u2 / rn, x3 = u3 / rn;
     T nrm = sqrt(x0 * x0 + x1 * x1 + x2 * x2 + x3 * x3);
@@ -194,7 +195,8 @@ __device__ __forceinline__ M3<T> rst_matrix(const T r[4], const T s[4], const T 
 
 template <typename T>
 __device__ __forceinline__ void draw_proposal(uint32_t k0, uint32_t k1, uint32_t link_id, uint32_t sweep,
-                                              uint32_t stream_id, int hit, T eps, T sq1me, M3<T> &X, double &r) {
+                                              uint32_t stream_id, int hit, T eps, T sq1me, bool flips, M3<T> &X,
+                                              double &r) {
     uint32_t w[8];
 #pragma unroll
     for (int call = 0; call < 2; call++) {
@@ -212,7 +214,7 @@ __device__ __forceinline__ void draw_proposal(uint32_t k0, uint32_t k1, uint32_t
             const uint32_t word = w[k >> 1];
             u[c] = su_scalar<T>(u_sym16((k & 1) ? (word >> 16) : (word & 0xFFFFu)));
         }
-        su2_near_unity<T>(u[0], u[1], u[2], u[3], eps, sq1me, su[b]);
+        su2_near_unity<T>(u[0], u[1], u[2], u[3], eps, sq1me, flips, su[b]);
     }
     X = rst_matrix<T>(su[0], su[1], su[2], (w[7] & 1u) == 0u);
     r = u_53(w[6], w[7]);
@@ -245,42 +247,75 @@ __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned lon
     }
 }
 
+// NUpdates hits on one link with staple A (GLAC/system.cpp:321-331): W = U A is
+// kept so a hit costs Re Tr(X W); returns the accepted count.
 template <typename T>
+__device__ __forceinline__ unsigned long long metropolis_hits(const LinkField<T> &L, int mu, int p, int s,
+                                                              const M3<T> &A, T mfac, T eps, T sq1me, bool flips,
+                                                              int nhits, uint32_t k0, uint32_t k1, uint32_t link_id,
+                                                              uint32_t sweep, uint32_t stream_id) {
+    M3<T> U = L.load_rw(mu, p, s);
+    M3<T> W = mul(U, A);
+    unsigned long long na = 0;
+#pragma unroll 1
+    for (int h = 0; h < nhits; h++) {
+        M3<T> X;
+        double r;
+        draw_proposal<T>(k0, k1, link_id, sweep, stream_id, h, eps, sq1me, flips, X, r);
+        const T dS = (retr_mul(X, W) - retr(W)) * mfac;
+        if (accept_weight<T>(dS) > r) {
+            U = mul(X, U);
+            W = mul(X, W);
+            na++;
+        }
+    }
+    L.store(mu, p, s, U);
+    return na;
+}
+
+// One (mu, parity) sub-sweep.  LEARNED: the spread of each link's proposals is
+// the network's output for its staple's features (every lane of the warp takes
+// part in the tensor-core inference; lanes past the plane pass zeros).
+template <typename T, bool LEARNED>
 __device__ __forceinline__ void metropolis_body(const Geom &g, const LinkField<T> &L, int mu, int p, T mfac, T eps,
                                                 T sq1me, int nhits, uint32_t k0, uint32_t k1, uint32_t sweep,
-                                                uint32_t stream_id, unsigned long long *acc) {
+                                                uint32_t stream_id, unsigned long long *acc, const Proposal &P,
+                                                float beta) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = s < g.Vh;
     unsigned long long na = 0;
-    if (s < g.Vh) {
+    if (LEARNED) {
+        __shared__ uint32_t feat[4 * 128];
+        float f[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        M3<T> A;
+        Site n;
+        if (valid) {
+            n = site_from_ps(g, p, s);
+            A = staple(L, g, n, p, mu);
+            staple_features(A, beta, f);
+        }
+        const float e = mlp_spread_warp(f, P, feat + (threadIdx.x >> 5) * 128);
+        if (valid) {
+            const T et = (T)e;
+            na = metropolis_hits<T>(L, mu, p, s, A, mfac, et, sqrt(T(1) - et * et), P.flips, nhits, k0, k1,
+                                    (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex, sweep, stream_id);
+        }
+    } else if (valid) {
         const Site n = site_from_ps(g, p, s);
         const M3<T> A = staple(L, g, n, p, mu);
-        M3<T> U = L.load_rw(mu, p, s);
-        M3<T> W = mul(U, A);
-        const uint32_t link_id = (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex;
-#pragma unroll 1
-        for (int h = 0; h < nhits; h++) {
-            M3<T> X;
-            double r;
-            draw_proposal<T>(k0, k1, link_id, sweep, stream_id, h, eps, sq1me, X, r);
-            const T dS = (retr_mul(X, W) - retr(W)) * mfac;
-            if (accept_weight<T>(dS) > r) {
-                U = mul(X, U);
-                W = mul(X, W);
-                na++;
-            }
-        }
-        L.store(mu, p, s, U);
+        na = metropolis_hits<T>(L, mu, p, s, A, mfac, eps, sq1me, P.flips, nhits, k0, k1,
+                                (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex, sweep, stream_id);
     }
     block_add_u64(na, acc);
 }
 
 #define GLAC_METRO_KERNEL(NAME, ATTR)                                                                        \
-    template <typename T>                                                                                  \
-    __global__ void ATTR NAME(Geom g, LinkField<T> L, int mu, int p, T mfac, T eps,                         \
-                                                     T sq1me, int nhits, uint32_t k0, uint32_t k1,          \
-                                                     uint32_t sweep, uint32_t stream_id,                    \
-                                                     unsigned long long *acc) {                             \
-        metropolis_body<T>(g, L, mu, p, mfac, eps, sq1me, nhits, k0, k1, sweep, stream_id, acc);           \
+    template <typename T, bool LEARNED>                                                                    \
+    __global__ void ATTR NAME(Geom g, LinkField<T> L, int mu, int p, T mfac, T eps, T sq1me, int nhits,      \
+                              uint32_t k0, uint32_t k1, uint32_t sweep, uint32_t stream_id,                 \
+                              unsigned long long *acc, Proposal P, float beta) {                            \
+        metropolis_body<T, LEARNED>(g, L, mu, p, mfac, eps, sq1me, nhits, k0, k1, sweep, stream_id, acc, P,  \
+                                    beta);                                                                 \
     }
 GLAC_METRO_KERNEL(k_metropolis, __launch_bounds__(128))
 GLAC_METRO_KERNEL(k_metropolis_r128, __maxnreg__(128))
@@ -288,25 +323,109 @@ GLAC_METRO_KERNEL(k_metropolis_r96, __maxnreg__(96))
 GLAC_METRO_KERNEL(k_metropolis_r80, __maxnreg__(80))
 #undef GLAC_METRO_KERNEL
 
+template <typename T, bool LEARNED>
+static void metro_dispatch(int regs, dim3 grid, cudaStream_t st, const Geom &g, const LinkField<T> &L, int mu,
+                           int p, T mfac, T e, T sq, int nhits, uint32_t k0, uint32_t k1, uint32_t sweep,
+                           uint32_t stream_id, unsigned long long *acc, const Proposal &P, float beta) {
+    switch (regs) {
+    case 128: k_metropolis_r128<T, LEARNED><<<grid, 128, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc, P, beta); break;
+    case 96: k_metropolis_r96<T, LEARNED><<<grid, 128, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc, P, beta); break;
+    case 80: k_metropolis_r80<T, LEARNED><<<grid, 128, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc, P, beta); break;
+    default: k_metropolis<T, LEARNED><<<grid, 128, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc, P, beta); break;
+    }
+}
+
 template <typename T>
 void launch_metropolis(const Geom &g, const LinkField<T> &L, int mu, int p, double beta, double eps, int nhits,
                        uint64_t seed, uint32_t sweep, uint32_t stream_id, unsigned long long *acc, int variant,
-                       cudaStream_t st) {
-    const int B = 128;
-    const dim3 grid((g.Vh + B - 1) / B);
+                       const Proposal &P, cudaStream_t st) {
+    const dim3 grid((g.Vh + 127) / 128);  // 128 threads: the learned path's shared memory holds 4 warps
     const T mfac = (T)(-beta / 3.0), e = (T)eps, sq = (T)sqrt(1.0 - eps * eps);
     const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-    switch (variant_regs(FAM_METRO, sizeof(T) == 4, variant)) {
-    case 128: k_metropolis_r128<T><<<grid, B, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc); break;
-    case 96: k_metropolis_r96<T><<<grid, B, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc); break;
-    case 80: k_metropolis_r80<T><<<grid, B, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc); break;
-    default: k_metropolis<T><<<grid, B, 0, st>>>(g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc); break;
-    }
+    const int regs = variant_regs(FAM_METRO, sizeof(T) == 4, variant);
+    if (P.net)
+        metro_dispatch<T, true>(regs, grid, st, g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc, P,
+                                (float)beta);
+    else
+        metro_dispatch<T, false>(regs, grid, st, g, L, mu, p, mfac, e, sq, nhits, k0, k1, sweep, stream_id, acc, P,
+                                 (float)beta);
 }
 template void launch_metropolis<double>(const Geom &, const LinkField<double> &, int, int, double, double, int,
-                                        uint64_t, uint32_t, uint32_t, unsigned long long *, int, cudaStream_t);
+                                        uint64_t, uint32_t, uint32_t, unsigned long long *, int, const Proposal &,
+                                        cudaStream_t);
 template void launch_metropolis<float>(const Geom &, const LinkField<float> &, int, int, double, double, int,
-                                       uint64_t, uint32_t, uint32_t, unsigned long long *, int, cudaStream_t);
+                                       uint64_t, uint32_t, uint32_t, unsigned long long *, int, const Proposal &,
+                                       cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Expected-squared-jump data for the learned spread (no reference counterpart).
+// Links s = offset + i stride (i < ns) of each (mu, parity) plane, rows in plane
+// order.  Per row: the staple's features, then for every eps_k on the grid the
+// mean over `trials` of ||U' - U||^2 = 6 - 2 Re Tr(X_acc) after the sampler's
+// nhits-hit update of that link (proposals from a Philox stream of their own:
+// stream | 2^31, sweep = snapshot, hit index h + 16 (trial + trials k)).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) k_esj(Geom g, LinkField<T> L, float beta, T mfac, int nhits, int n_eps,
+                                             const float *__restrict__ eps_grid, int trials, int stride, int offset,
+                                             int ns, uint32_t k0, uint32_t k1, uint32_t snapshot, uint32_t stream_id,
+                                             bool flips, float *__restrict__ feat, float *__restrict__ esj,
+                                             uint32_t *__restrict__ ids) {
+    const long long row = (long long)blockIdx.x * 128 + threadIdx.x;
+    if (row >= 8ll * ns) return;
+    const int plane = (int)(row / ns), i = (int)(row % ns);
+    const int mu = plane >> 1, p = plane & 1, s = offset + i * stride;
+    const Site n = site_from_ps(g, p, s);
+    const M3<T> A = staple(L, g, n, p, mu);
+    float f[8];
+    staple_features(A, beta, f);
+    float4 *fo = reinterpret_cast<float4 *>(feat + row * 8);
+    fo[0] = make_float4(f[0], f[1], f[2], f[3]);
+    fo[1] = make_float4(f[4], f[5], f[6], f[7]);
+    const uint32_t link_id = (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex;
+    if (ids) ids[row] = link_id;
+    if (n_eps == 0) return;
+    const M3<T> W0 = mul(L.load(mu, p, s), A);
+    for (int k = 0; k < n_eps; k++) {
+        const T eps = (T)eps_grid[k], sq = sqrt(T(1) - eps * eps);
+        T J = T(0);
+        for (int tr = 0; tr < trials; tr++) {
+            M3<T> Xt, Wc = W0;
+            set_identity(Xt);
+#pragma unroll 1
+            for (int h = 0; h < nhits; h++) {
+                M3<T> X;
+                double r;
+                draw_proposal<T>(k0, k1, link_id, snapshot, stream_id, h + 16 * (tr + trials * k), eps, sq, flips, X,
+                                 r);
+                const T dS = (retr_mul(X, Wc) - retr(Wc)) * mfac;
+                if (accept_weight<T>(dS) > r) {
+                    Xt = mul(X, Xt);
+                    Wc = mul(X, Wc);
+                }
+            }
+            J += T(6) - T(2) * retr(Xt);
+        }
+        esj[row * n_eps + k] = (float)(J / T(trials));
+    }
+}
+
+template <typename T>
+void launch_esj(const Geom &g, const LinkField<T> &L, double beta, int nhits, int n_eps, const float *eps_grid_dev,
+                int trials, int stride, int offset, int ns, uint64_t seed, uint32_t snapshot, uint32_t stream_id,
+                bool flips, float *feat, float *esj, uint32_t *ids, cudaStream_t st) {
+    const long long rows = 8ll * ns;
+    k_esj<T><<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(g, L, (float)beta, (T)(-beta / 3.0), nhits, n_eps,
+                                                            eps_grid_dev, trials, stride, offset, ns, (uint32_t)seed,
+                                                            (uint32_t)(seed >> 32), snapshot,
+                                                            stream_id | 0x80000000u, flips, feat, esj, ids);
+}
+template void launch_esj<double>(const Geom &, const LinkField<double> &, double, int, int, const float *, int, int,
+                                 int, int, uint64_t, uint32_t, uint32_t, bool, float *, float *, uint32_t *,
+                                 cudaStream_t);
+template void launch_esj<float>(const Geom &, const LinkField<float> &, double, int, int, const float *, int, int,
+                                int, int, uint64_t, uint32_t, uint32_t, bool, float *, float *, uint32_t *,
+                                cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Observables (GLAC/observables/mastersamplertopcxyz.cpp:236-384): per site,
@@ -586,7 +705,7 @@ __global__ void k_rst_start(Geom g, LinkField<T> L, double eps, uint32_t k0, uin
     M3<double> X;
     double r;
     draw_proposal<double>(k0, k1, (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex, 0xFFFFFFFFu, stream_id, 0, eps,
-                          sqrt(1.0 - eps * eps), X, r);
+                          sqrt(1.0 - eps * eps), true, X, r);
     L.store(mu, p, s, to_t<T>(X));
 }
 template <typename T>

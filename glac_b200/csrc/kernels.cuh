@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "lattice.cuh"
+#include "learned.cuh"
 #include "expm.cuh"
 
 namespace glac {
@@ -63,10 +64,16 @@ int variant_shape(Family f, bool fp32, int v);  // flow site-block shape of a va
 template <typename T>
 void launch_flow_stage(const Geom &g, const LinkField<T> &in, const LinkField<T> &out, const ForceField<T> &zf,
                        int stage, int kind, double alpha, double beta, int variant, cudaStream_t st);
+// P.net set: the learned spread (learned.cuh) replaces eps per link.
 template <typename T>
 void launch_metropolis(const Geom &g, const LinkField<T> &L, int mu, int p, double beta, double eps, int nhits,
                        uint64_t seed, uint32_t sweep, uint32_t stream_id, unsigned long long *acc, int variant,
-                       cudaStream_t st);
+                       const Proposal &P, cudaStream_t st);
+// Expected-squared-jump rows of 8 * ns sampled links (features [row][8], esj [row][n_eps], ids [row] or null).
+template <typename T>
+void launch_esj(const Geom &g, const LinkField<T> &L, double beta, int nhits, int n_eps, const float *eps_grid_dev,
+                int trials, int stride, int offset, int ns, uint64_t seed, uint32_t snapshot, uint32_t stream_id,
+                bool flips, float *feat, float *esj, uint32_t *ids, cudaStream_t st);
 template <typename T>
 void launch_observables(const Geom &g, const LinkField<T> &L, const ObsPlan &plan, double *partial,
                         double *out, int variant, cudaStream_t st);

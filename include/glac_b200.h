@@ -71,7 +71,12 @@ void *glac_stream(glac_ctx *ctx);
 glac_status glac_sync(glac_ctx *ctx);
 /* Number of kernels this context has launched so far. */
 uint64_t glac_launch_count(const glac_ctx *ctx);
-/* Tuning switches by name (none defined at present; unknown keys give GLAC_ERR_ARG). */
+/* Switches by name; unknown keys give GLAC_ERR_ARG.
+ *   "su2_sign_flips" (default 1): 1 draws the SU(2) factors of each proposal as
+ *   the reference does, x0 = sign(u0) sqrt(1 - eps^2)
+ *   (su3matrixgenerator.h:202-243); 0 keeps x0 = +sqrt(1 - eps^2), every factor
+ *   near the identity (a symmetric proposal as well; no reference counterpart).
+ *   Applies to glac_metropolis and glac_esj_data. */
 glac_status glac_set_option(glac_ctx *ctx, const char *key, long value);
 
 /* ---- field --------------------------------------------------------------- */
@@ -171,6 +176,63 @@ glac_status glac_accept_fed(int precision, double beta, long n_links, int n_hits
  * glac_noalloc_error(). */
 glac_status glac_measure_noalloc(const int dims[4], const double *dev_links, double *dev_obs, void *stream);
 const char *glac_noalloc_error(void);
+
+/* ---- learned proposal spread (no counterpart in the reference) ---------- */
+/* The reference draws every proposal with the run-config's SU3Eps
+ * (su3matrixgenerator.cpp:16-35).  Here a small network may choose the spread
+ * of each link's proposals from eight gauge-invariant features of its staple;
+ * the staple does not change when its own link is updated, so the proposal
+ * stays symmetric and the accept step (system.cpp:333-361) stays exact.
+ * Network: 8 -> 32 -> 32 -> 1, leaky ReLU (slope 1/16), eps = eps_min +
+ * (eps_max - eps_min) sigmoid(z); BF16 operands, FP32 accumulation.
+ * Parameters, GLAC_MLP_NPARAMS floats, flat: W1[8][32], b1[32], W2[32][32],
+ * b2[32], W3[32], b3 (x W1 + b1, row-vector convention). */
+#define GLAC_MLP_NPARAMS 1377
+
+/* Use the network for this context's Metropolis proposals from now on
+ * (params = NULL: back to the fixed spread su3_eps).  0 < eps_min < eps_max <= 1. */
+glac_status glac_set_proposal_net(glac_ctx *ctx, const float *params, double eps_min,
+                                  double eps_max);
+
+/* Expected-squared-jump training data from the current field.  Samples the
+ * links s = o + i*stride (i < V/2/stride, o = snapshot*7919 mod stride) of each
+ * (mu, parity) plane: rows = 8 * (V/2 / stride), written to *n_rows.  Per row:
+ * dev_features[row*8 .. +8] = the staple's features; for each of the n_eps
+ * spreads, dev_esj[row*n_eps + k] = mean over `trials` of ||U' - U||^2 after
+ * n_updates Metropolis hits of that link with spread eps_grid[k] (its own
+ * Philox stream, so the chain's draws are untouched; the field is not
+ * modified); dev_link_ids[row] = mu*V + site (may be NULL).  n_eps = 0 gives
+ * the features alone.  Device pointers; capacity = rows the buffers hold.
+ * Synchronous. */
+glac_status glac_esj_data(glac_ctx *ctx, int n_eps, const double *eps_grid, int trials, int stride,
+                          uint32_t snapshot, float *dev_features, float *dev_esj, uint32_t *dev_link_ids,
+                          long long capacity, long long *n_rows);
+
+/* Trainer: FP32 master parameters with Adam state on one device; forward and
+ * backward passes on the tensor cores.  Device-pointer inputs must be ready
+ * (their producers synchronised) before each call; every call is synchronous. */
+typedef struct glac_mlp glac_mlp;
+glac_status glac_mlp_create(int device, glac_mlp **out);
+void glac_mlp_destroy(glac_mlp *mlp);
+const char *glac_mlp_last_error(const glac_mlp *mlp);
+/* Set / read the GLAC_MLP_NPARAMS parameters (setting resets Adam). */
+glac_status glac_mlp_set_params(glac_mlp *mlp, const float *host_params);
+glac_status glac_mlp_get_params(glac_mlp *mlp, float *host_params);
+/* He-normal initialisation from seed with the output bias at spread eps0. */
+glac_status glac_mlp_init(glac_mlp *mlp, uint64_t seed, double eps_min, double eps_max, double eps0);
+/* dev_eps[i] = spread for dev_features[i*8 .. +8], i < n. */
+glac_status glac_mlp_forward(glac_mlp *mlp, const float *dev_features, long long n, double eps_min, double eps_max,
+                             float *dev_eps);
+/* Loss L = -(1/n) sum_i J_i(eps_i), J_i linear between the n_eps grid points
+ * (eps_min, eps_max = the grid's ends) over rows dev_esj[i*n_eps ..], and its
+ * gradient (host_grad may be NULL).  Deterministic for a given n. */
+glac_status glac_mlp_loss_grad(glac_mlp *mlp, const float *dev_features, const float *dev_esj, long long n,
+                               int n_eps, const double *eps_grid, double *loss, float *host_grad);
+/* `steps` Adam steps (learning rate lr) on consecutive batches of `batch` rows,
+ * cycling over the n rows in order; host_losses[steps] (may be NULL) receives
+ * the loss of each step's batch before its update. */
+glac_status glac_mlp_train(glac_mlp *mlp, const float *dev_features, const float *dev_esj, long long n, int n_eps,
+                           const double *eps_grid, int steps, long long batch, double lr, double *host_losses);
 
 /* ---- gauge-field files (GLAC/io/fieldio.cpp) ----------------------------- */
 /* Read a GLAC .bin configuration (per site 4 links x 18 doubles, x fastest;

@@ -501,7 +501,7 @@ static double u_53(uint32_t hi, uint32_t lo) {
  * (su3matrixgenerator.h:170-196), words 6-7 the 53-bit accept uniform, and bit
  * 0 of word 7 chooses X or X^+. */
 static void proposal(uint32_t key[2], uint32_t link_id, uint32_t sweep, uint32_t stream, int hit,
-                     double eps, double *X, double *r) {
+                     double eps, int flips, double *X, double *r) {
     uint32_t w[8];
     for (int call = 0; call < 2; call++) {
         uint32_t ctr[4] = {(uint32_t)(2 * hit + call), link_id, sweep, stream};
@@ -515,6 +515,7 @@ static void proposal(uint32_t key[2], uint32_t link_id, uint32_t sweep, uint32_t
             uint32_t word = w[k >> 1];
             u[c] = u_sym16((k & 1) ? (word >> 16) : (word & 0xFFFFu));
         }
+        if (!flips) u[0] = fabs(u[0]); /* x0 = +sqrt(1 - eps^2): every factor near the identity */
         oracle_su2_near_unity(u, eps, su2[b]);
     }
     int inverse = (w[7] & 1u) == 0u;
@@ -523,7 +524,7 @@ static void proposal(uint32_t key[2], uint32_t link_id, uint32_t sweep, uint32_t
 }
 
 uint64_t oracle_metropolis_sweep(const int N[4], double *links, double beta, double eps,
-                                 int nhits, uint64_t seed, uint32_t stream, uint32_t sweep) {
+                                 int nhits, uint64_t seed, uint32_t stream, uint32_t sweep, int flips) {
     long V = (long)N[0] * N[1] * N[2] * N[3];
     uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
     uint64_t accepted = 0;
@@ -538,7 +539,7 @@ uint64_t oracle_metropolis_sweep(const int N[4], double *links, double beta, dou
             double *u = LINK(links, V, mu, s);
             for (int h = 0; h < nhits; h++) {
                 double X[18], Up[18], r;
-                proposal(key, (uint32_t)(mu * V + s), sweep, stream, h, eps, X, &r);
+                proposal(key, (uint32_t)(mu * V + s), sweep, stream, h, eps, flips, X, &r);
                 mm(X, u, Up);
                 if (exp(-oracle_delta_s(u, Up, A, beta)) > r) {
                     memcpy(u, Up, sizeof(Up));
@@ -548,6 +549,41 @@ uint64_t oracle_metropolis_sweep(const int N[4], double *links, double beta, dou
         }
     }
     return accepted;
+}
+
+/* Expected squared jump of one link (project design, the learned-spread
+ * training data): for each spread eps_grid[k], the mean over `trials` of
+ * ||U' - U||^2 = 6 - 2 ReTr(X_acc) after nhits Metropolis hits with staple A
+ * (accept iff exp(-dS) > r, dS = -(beta/3)(ReTr(X W) - ReTr W), W = current
+ * link times A), proposals from stream | 2^31 with sweep = snapshot and hit
+ * index h + 16 (trial + trials k); flips = 0 draws every SU(2) factor near +1. */
+void oracle_esj_link(const double *U, const double *A, double beta, int nhits, int n_eps, const double *eps_grid,
+                     int trials, uint64_t seed, uint32_t link_id, uint32_t snapshot, uint32_t stream, int flips,
+                     double *J) {
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    double W0[18];
+    mm(U, A, W0);
+    for (int k = 0; k < n_eps; k++) {
+        double acc = 0.0;
+        for (int tr = 0; tr < trials; tr++) {
+            double Xt[18], Wc[18], X[18], T[18], r;
+            mident(Xt);
+            memcpy(Wc, W0, sizeof(Wc));
+            for (int h = 0; h < nhits; h++) {
+                proposal(key, link_id, snapshot, stream | 0x80000000u, h + 16 * (tr + trials * k), eps_grid[k], flips,
+                         X, &r);
+                double dS = -(beta / 3.0) * (retr_mul(X, Wc) - retr(Wc));
+                if (exp(-dS) > r) {
+                    mm(X, Xt, T);
+                    memcpy(Xt, T, sizeof(T));
+                    mm(X, Wc, T);
+                    memcpy(Wc, T, sizeof(T));
+                }
+            }
+            acc += 6.0 - 2.0 * retr(Xt);
+        }
+        J[k] = acc / trials;
+    }
 }
 
 void oracle_haar_field(const int N[4], double *links, uint64_t seed, uint32_t stream) {

@@ -72,9 +72,16 @@ void oracle_accept_fed(long nlinks, int nhits, double beta, double *U, const dou
  * counterpart): sub-sweep k = 2*mu + parity; for each link of that class the
  * staple is taken once and nhits proposals drawn from the Philox stream
  * (key = seed, counter = {2*hit + call, mu*V + site, sweep, stream}).
+ * flips = 0 draws every SU(2) factor near +1 (x0 > 0), 1 as the reference.
  * Returns accepted proposals; links updated in place. */
 uint64_t oracle_metropolis_sweep(const int N[4], double *links, double beta, double eps,
-                                 int nhits, uint64_t seed, uint32_t stream, uint32_t sweep);
+                                 int nhits, uint64_t seed, uint32_t stream, uint32_t sweep, int flips);
+
+/* Expected squared jump of one link for each spread on a grid (project design,
+ * training data of the learned proposal spread); see glac_oracle.c. */
+void oracle_esj_link(const double *U, const double *A, double beta, int nhits, int n_eps, const double *eps_grid,
+                     int trials, uint64_t seed, uint32_t link_id, uint32_t snapshot, uint32_t stream, int flips,
+                     double *J);
 
 /* Seeded Haar-random SU(3) field (QR of a complex Gaussian matrix with phase fix,
  * then det normalisation), 4V links; counter = {call, mu*V + site, 0xA11A, stream}. */

@@ -73,10 +73,12 @@ class Oracle:
         lib.oracle_su2_near_unity.argtypes = [_dp, C.c_double, _dp]
         lib.oracle_accept_fed.argtypes = [C.c_long, C.c_int, C.c_double, _dp, _dp, _dp, _dp, _u8]
         lib.oracle_metropolis_sweep.argtypes = [C.c_int * 4, _dp, C.c_double, C.c_double, C.c_int,
-                                                C.c_uint64, C.c_uint32, C.c_uint32]
+                                                C.c_uint64, C.c_uint32, C.c_uint32, C.c_int]
         lib.oracle_metropolis_sweep.restype = C.c_uint64
         lib.oracle_haar_field.argtypes = [C.c_int * 4, _dp, C.c_uint64, C.c_uint32]
         lib.oracle_reunitarize.argtypes = [_dp, C.c_long]
+        lib.oracle_esj_link.argtypes = [_dp, _dp, C.c_double, C.c_int, C.c_int, _dp, C.c_int, C.c_uint64,
+                                        C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, _dp]
         self.lib = lib
 
     def philox(self, ctr, key):
@@ -150,11 +152,20 @@ class Oracle:
                                    np.ascontiguousarray(X, np.float64), np.ascontiguousarray(r, np.float64), acc)
         return U, acc.reshape(nl, nh)
 
-    def metropolis_sweep(self, N, links, beta, eps, nhits, seed, stream, sweep):
+    def metropolis_sweep(self, N, links, beta, eps, nhits, seed, stream, sweep, flips=True):
         n, _ = _dims(N)
         out = np.array(links, np.float64, copy=True, order="C")
-        acc = self.lib.oracle_metropolis_sweep(n, out, beta, eps, nhits, seed, stream, sweep)
+        acc = self.lib.oracle_metropolis_sweep(n, out, beta, eps, nhits, seed, stream, sweep, int(bool(flips)))
         return out, int(acc)
+
+    def esj_link(self, U, A, beta, nhits, eps_grid, trials, seed, link_id, snapshot, stream, flips=True):
+        """Expected squared jump of one link for each spread on the grid."""
+        g = np.ascontiguousarray(eps_grid, np.float64)
+        J = np.zeros(g.size)
+        self.lib.oracle_esj_link(np.ascontiguousarray(U, np.float64), np.ascontiguousarray(A, np.float64),
+                                 float(beta), int(nhits), g.size, g, int(trials), int(seed), int(link_id),
+                                 int(snapshot), int(stream), int(bool(flips)), J)
+        return J
 
     def haar_field(self, N, seed, stream=0):
         n, V = _dims(N)

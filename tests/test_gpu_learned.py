@@ -1,0 +1,188 @@
+"""GPU tests of the learned proposal spread, through the C ABI.
+
+* features and expected-squared-jump data of the kernels against the oracle
+  (oracle/mlp.py, oracle_esj_link);
+* the tensor-core forward pass and gradient against the oracle's BF16-emulating
+  restatement; training on the GPU reaches a known optimum;
+* exactness: a chain whose spread varies link by link with the staple still
+  reproduces the reference's ensemble plaquette;
+* what the network gains over the fixed spread on held-out data.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mlp
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def g():
+    import glac_b200
+    return glac_b200
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+@pytest.fixture(scope="module")
+def learned():
+    from glac_b200 import learned
+    return learned
+
+
+def f32(a):
+    return np.asarray(a, np.float32).astype(np.float64)
+
+
+def random_params(seed, w3=0.3, b3=-0.5):
+    rng = np.random.default_rng(seed)
+    P = np.zeros(mlp.NPARAMS)
+    P[mlp.W1:mlp.B1] = rng.standard_normal(256) * 0.5
+    P[mlp.B1:mlp.W2] = rng.standard_normal(32) * 0.1
+    P[mlp.W2:mlp.B2] = rng.standard_normal(1024) * 0.25
+    P[mlp.B2:mlp.W3] = rng.standard_normal(32) * 0.1
+    P[mlp.W3:mlp.B3] = rng.standard_normal(32) * w3
+    P[mlp.B3] = b3
+    return P.astype(np.float32)
+
+
+def esj_rows(g, torch, L, grid, trials, stride, snapshot):
+    rows = L.esj_rows(stride)
+    feat = torch.empty((rows, 8), dtype=torch.float32, device="cuda")
+    esj = torch.empty((rows, max(len(grid), 1)), dtype=torch.float32, device="cuda")
+    ids = torch.empty(rows, dtype=torch.int32, device="cuda")
+    n = L.esj_data_ptr(grid, trials, stride, snapshot, feat.data_ptr(), esj.data_ptr(), ids.data_ptr(), rows)
+    assert n == rows
+    return feat.cpu().numpy(), esj.cpu().numpy(), ids.cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-6), ("fp32", 3e-4)])
+def test_features_match_oracle(g, torch, oracle, prec, tol):
+    N, V = (4, 4, 4, 8), 512
+    links = oracle.haar_field(N, 11)
+    with g.Lattice(N, beta=6.0, precision=prec) as L:
+        L.set_links(links)
+        feat, _, ids = esj_rows(g, torch, L, [], 1, 1, 0)
+    assert np.array_equal(np.sort(ids), np.arange(4 * V))
+    want = mlp.features(oracle.staples(N, links).reshape(-1, 18)[ids], 6.0)
+    assert np.max(np.abs(feat - want) / (1 + np.abs(want))) < tol
+
+
+@pytest.mark.parametrize("prec,flips", [("fp64", True), ("fp64", False), ("fp32", False)])
+def test_esj_matches_oracle(g, torch, oracle, prec, flips):
+    N, V, beta, seed, stream = (4, 4, 4, 8), 512, 6.0, 77, 3
+    links = oracle.haar_field(N, 12)
+    for sw in range(6):  # off the Haar start, so that a fair share of moves is accepted
+        links, _ = oracle.metropolis_sweep(N, links, beta, 0.24, 10, 5, 0, sw)
+    grid = f32(np.geomspace(0.03, 0.9, 8))
+    with g.Lattice(N, beta=beta, precision=prec, seed=seed, stream_id=stream) as L:
+        L.set_links(links)
+        L.set_option("su2_sign_flips", int(flips))
+        feat, esj, ids = esj_rows(g, torch, L, grid, 3, 4, 5)
+    A = oracle.staples(N, links).reshape(-1, 18)
+    U = links.reshape(-1, 18)
+    want = np.array([oracle.esj_link(U[i], A[i], beta, 10, grid, 3, seed, i, 5, stream, flips) for i in ids])
+    d = np.abs(esj - want)
+    assert want.mean() > 0.01  # moves get accepted: the comparison is not trivial
+    if prec == "fp64":  # the rows are stored as float32
+        assert np.all(d <= 1.2e-7 * np.abs(want) + 1e-12)
+    else:  # FP32: the same draws; an accept decision at the threshold may flip
+        assert np.mean(d < 1e-4) > 0.97
+        assert abs(esj.mean() - want.mean()) < 0.01 * want.mean()
+
+
+def test_forward_matches_oracle(g, torch, learned):
+    rng = np.random.default_rng(1)
+    X = rng.standard_normal((3000, 8)).astype(np.float32)
+    P = random_params(2)
+    with learned.ProposalNet() as net:
+        net.params = P
+        got = net.forward(torch.from_numpy(X).cuda(), 0.03, 0.9).cpu().numpy()
+    want = mlp.spread(P, X, f32(0.03)[()], f32(0.9)[()], emulate=True)
+    d = np.abs(got - want)
+    assert np.median(d) < 1e-5 and d.max() < 5e-3
+    assert got.std() > 0.05  # the spread really varies with the features
+
+
+def test_gradient_matches_oracle(g, torch, learned):
+    rng = np.random.default_rng(3)
+    n, K = 5000, 16
+    X = rng.standard_normal((n, 8)).astype(np.float32)
+    grid = f32(np.geomspace(0.03, 0.9, K))
+    J = (np.abs(rng.standard_normal((n, K))) * np.sin(np.pi * grid)[None, :]).astype(np.float32)
+    P = random_params(4)
+    with learned.ProposalNet() as net:
+        net.params = P
+        loss, grad = net.loss_grad(torch.from_numpy(X).cuda(), torch.from_numpy(J).cuda(), grid)
+        # deterministic: the same call gives the same bits
+        loss2, grad2 = net.loss_grad(torch.from_numpy(X).cuda(), torch.from_numpy(J).cuda(), grid)
+    assert loss == loss2 and np.array_equal(grad, grad2)
+    lo, go = mlp.loss_grad(P.astype(np.float64), X, J, grid, emulate=True)
+    assert abs(loss - lo) < 1e-4 * abs(lo)
+    for a, b in ((mlp.W1, mlp.B1), (mlp.B1, mlp.W2), (mlp.W2, mlp.B2), (mlp.B2, mlp.W3), (mlp.W3, mlp.NPARAMS)):
+        assert np.linalg.norm(grad[a:b] - go[a:b]) < 0.02 * np.linalg.norm(go[a:b]) + 1e-7, (a, b)
+
+
+def test_training_finds_known_optimum(g, torch, learned):
+    # J_i(eps) peaks at eps*(x_i) = 0.1 + 0.5 sigmoid(2 x_i0): the trained spread must follow it
+    rng = np.random.default_rng(5)
+    n, grid = 65536, f32(np.geomspace(0.03, 0.9, 24))
+    X = rng.standard_normal((n, 8)).astype(np.float32)
+    target = 0.1 + 0.5 / (1 + np.exp(-2 * X[:, 0]))
+    J = np.exp(-((grid[None, :] - target[:, None]) / 0.15) ** 2).astype(np.float32)
+    with learned.ProposalNet() as net:
+        net.init(9, grid[0], grid[-1], 0.24)
+        Xd, Jd = torch.from_numpy(X).cuda(), torch.from_numpy(J).cuda()
+        losses = net.train(Xd, Jd, grid, 1500, 4096, 3e-3)
+        eps = net.forward(Xd, grid[0], grid[-1]).cpu().numpy()
+    assert losses[-100:].mean() < 0.8 * losses[:10].mean()
+    assert np.mean(np.abs(eps - target)) < 0.03
+
+
+def test_learned_chain_keeps_reference_plaquette(g):
+    # A spread that varies over [0.1, 0.6] link by link with the staple, with
+    # every SU(2) factor near +1, must leave the equilibrium unchanged.  Each
+    # chain is thermalised like the reference's (Haar start, 200 plain sweeps),
+    # then continues with the learned proposal for the measured sweeps.
+    with open(os.path.join(HERE, "golden", "ensemble_4x4x4x8_b6.json")) as f:
+        ref = json.load(f)
+    from glac_b200.analysis import binned_mean
+    P = random_params(6, w3=0.6, b3=0.0)
+    plaqs, spreads = [], []
+    for i in range(8):
+        with g.Lattice(tuple(ref["lattice"]), beta=ref["beta"], precision="fp32", seed=900 + i) as L:
+            L.hot_start(300 + i)
+            L.metropolis(ref["therm_sweeps"])
+            L.set_option("su2_sign_flips", 0)
+            L.set_proposal_net(P, 0.1, 0.6)
+            p = np.empty(ref["meas_sweeps"])
+            for k in range(p.size):
+                L.metropolis(1)
+                p[k] = L.measure()[0]
+            plaqs.append(p)
+    mean, err = binned_mean(plaqs, 20)
+    sigma = np.hypot(err, ref["plaquette_error"])
+    assert abs(mean - ref["plaquette"]) < 3 * sigma, (mean, err, ref["plaquette"])
+
+
+def test_trained_spread_beats_fixed_spread(g, torch, learned):
+    grid = learned.DEFAULT_GRID
+    with g.Lattice((8, 8, 8, 16), beta=6.0, precision="fp32", seed=3) as L:
+        L.hot_start(3)
+        L.metropolis(300)
+        feat, esj, plain = learned.collect_esj(L, 200, 10, 2, grid, trials=4)
+    net, rep = learned.train_proposal(feat, esj, grid, steps=800, batch=4096, lr=3e-3, seed=1, esj_plain=plain)
+    net.close()
+    # held-out rows: mean squared jump per link update of the trained network
+    # against the reference's proposal (eps = 0.24) and the family's fixed spreads
+    assert rep["gain_vs_plain"] > 1.5, rep
+    assert rep["gain_vs_024"] > 1.05, rep
+    assert rep["gain_vs_best_fixed"] > 0.99, rep

@@ -198,15 +198,17 @@ def test_accept_decisions_full_reference_sweep(g, oracle, reference):
     assert rel_err(final, tr["links"]) < 1e-13
 
 
-def test_checkerboard_sweep_matches_oracle(g, oracle):
+@pytest.mark.parametrize("flips", [True, False])
+def test_checkerboard_sweep_matches_oracle(g, oracle, flips):
     N = (4, 4, 4, 8)
     start = oracle.haar_field(N, 7)
     with lattice(g, N, "fp64", beta=6.0, su3_eps=0.24, n_updates=10, seed=0x1234_5678_9ABC, stream_id=3) as L:
         L.set_links(start)
+        L.set_option("su2_sign_flips", int(flips))
         ref = start
         total = 0
         for sweep in range(3):
-            ref, a = oracle.metropolis_sweep(N, ref, 6.0, 0.24, 10, 0x1234_5678_9ABC, 3, sweep)
+            ref, a = oracle.metropolis_sweep(N, ref, 6.0, 0.24, 10, 0x1234_5678_9ABC, 3, sweep, flips)
             total += a
         acc = L.metropolis(3)
         assert abs(acc * 4 * 10 * L.V * 3 - total) < 0.5
