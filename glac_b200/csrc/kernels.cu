@@ -29,9 +29,9 @@ namespace glac {
 //            are re-read from L1.
 template <typename T, int KIND, int STAGE, int SHAPE>
 __device__ __forceinline__ void flow_stage_body(const Geom &g, const LinkField<T> &in, const LinkField<T> &out,
-                                                const ForceField<T> &zf, T alpha, T beta) {
-    const int plane = SHAPE == 1 ? int(threadIdx.x >> 4) : int(blockIdx.x & 7);
-    const int s = SHAPE == 1 ? int(blockIdx.x * 16 + (threadIdx.x & 15)) : int((blockIdx.x >> 3) * 128 + threadIdx.x);
+                                                const ForceField<T> &zf, T alpha, T beta, int bx) {
+    const int plane = SHAPE == 1 ? int(threadIdx.x >> 4) : (bx & 7);
+    const int s = SHAPE == 1 ? int(bx * 16 + (threadIdx.x & 15)) : int((bx >> 3) * 128 + threadIdx.x);
     if (s >= g.Vh) return;
     const int mu = plane >> 1, p = plane & 1;
     const Site n = site_from_ps(g, p, s);
@@ -62,7 +62,7 @@ __device__ __forceinline__ void flow_stage_body(const Geom &g, const LinkField<T
     template <typename T, int KIND, int STAGE, int SHAPE>                                                \
     __global__ void ATTR NAME(Geom g, LinkField<T> in, LinkField<T> out, ForceField<T> zf, T alpha,      \
                               T beta) {                                                                  \
-        flow_stage_body<T, KIND, STAGE, SHAPE>(g, in, out, zf, alpha, beta);                             \
+        flow_stage_body<T, KIND, STAGE, SHAPE>(g, in, out, zf, alpha, beta, blockIdx.x);                 \
     }
 GLAC_FLOW_KERNEL(k_flow_stage, __launch_bounds__(128))
 GLAC_FLOW_KERNEL(k_flow_stage_r128, __maxnreg__(128))
@@ -280,8 +280,8 @@ template <typename T, bool LEARNED>
 __device__ __forceinline__ void metropolis_body(const Geom &g, const LinkField<T> &L, int mu, int p, T mfac, T eps,
                                                 T sq1me, int nhits, uint32_t k0, uint32_t k1, uint32_t sweep,
                                                 uint32_t stream_id, unsigned long long *acc, const Proposal &P,
-                                                float beta) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+                                                float beta, int bx) {
+    const int s = bx * blockDim.x + threadIdx.x;
     const bool valid = s < g.Vh;
     unsigned long long na = 0;
     if (LEARNED) {
@@ -315,7 +315,7 @@ __device__ __forceinline__ void metropolis_body(const Geom &g, const LinkField<T
                               uint32_t k0, uint32_t k1, uint32_t sweep, uint32_t stream_id,                 \
                               unsigned long long *acc, Proposal P, float beta) {                            \
         metropolis_body<T, LEARNED>(g, L, mu, p, mfac, eps, sq1me, nhits, k0, k1, sweep, stream_id, acc, P,  \
-                                    beta);                                                                 \
+                                    beta, blockIdx.x);                                                     \
     }
 GLAC_METRO_KERNEL(k_metropolis, __launch_bounds__(128))
 GLAC_METRO_KERNEL(k_metropolis_r128, __maxnreg__(128))
@@ -527,8 +527,7 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 
 template <typename T>
 __device__ __forceinline__ void observables_body(const Geom &g, const LinkField<T> &L, int nb, int Bv,
-                                                 double *partial) {
-    const int b = blockIdx.x;
+                                                 double *partial, int b) {
     const int t = b / (2 * nb);
     const int p = (b / nb) & 1;
     const int j = b % nb;
@@ -570,7 +569,7 @@ __device__ __forceinline__ void observables_body(const Geom &g, const LinkField<
 #define GLAC_OBS_KERNEL(NAME, ATTR)                                                                      \
     template <typename T>                                                                              \
     __global__ void ATTR NAME(Geom g, LinkField<T> L, int nb, int Bv, double *partial) {               \
-        observables_body<T>(g, L, nb, Bv, partial);                                                    \
+        observables_body<T>(g, L, nb, Bv, partial, blockIdx.x);                                        \
     }
 GLAC_OBS_KERNEL(k_observables, __launch_bounds__(256))
 GLAC_OBS_KERNEL(k_observables_r128, __maxnreg__(128))
@@ -579,7 +578,7 @@ GLAC_OBS_KERNEL(k_observables_r96, __maxnreg__(96))
 
 // out = [plaq, topc, energy, topct[Nt]] with the reference's normalisations
 // (mastersamplertopcxyz.cpp:13-16, :363-383).
-__global__ void k_obs_finalize(int Nt, int nb, int V, const double *partial, double *out) {
+__device__ __forceinline__ void obs_finalize_body(int Nt, int nb, int V, const double *partial, double *out) {
     __shared__ double sp[1024], se[1024], sq[1024];
     for (int t = threadIdx.x; t < Nt; t += blockDim.x) {
         double a = 0.0, e = 0.0, q = 0.0;
@@ -601,6 +600,9 @@ __global__ void k_obs_finalize(int Nt, int nb, int V, const double *partial, dou
         out[2] = e / (double)V;
         for (int t = 0; t < Nt; t++) out[3 + t] = sq[t] * qfac;
     }
+}
+__global__ void k_obs_finalize(int Nt, int nb, int V, const double *partial, double *out) {
+    obs_finalize_body(Nt, nb, V, partial, out);
 }
 
 template <typename T>
@@ -637,10 +639,8 @@ template <typename T> __device__ __forceinline__ M3<double> to_d(const M3<T> &a)
 
 // grid: x over Vh, y = mu*2 + parity
 template <typename T>
-__global__ void k_haar(Geom g, LinkField<T> L, uint32_t k0, uint32_t k1, uint32_t stream_id) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= g.Vh) return;
-    const int mu = blockIdx.y >> 1, p = blockIdx.y & 1;
+__device__ __forceinline__ void haar_link(const Geom &g, const LinkField<T> &L, int mu, int p, int s, uint32_t k0,
+                                          uint32_t k1, uint32_t stream_id) {
     const Site n = site_from_ps(g, p, s);
     const uint32_t link_id = (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex;
     uint32_t w[20];
@@ -690,6 +690,12 @@ __global__ void k_haar(Geom g, LinkField<T> L, uint32_t k0, uint32_t k1, uint32_
 #pragma unroll
     for (int e = 0; e < 9; e++) Z.e[e] = Z.e[e] * f;
     L.store(mu, p, s, to_t<T>(Z));
+}
+template <typename T>
+__global__ void k_haar(Geom g, LinkField<T> L, uint32_t k0, uint32_t k1, uint32_t stream_id) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.Vh) return;
+    haar_link(g, L, blockIdx.y >> 1, blockIdx.y & 1, s, k0, k1, stream_id);
 }
 
 // Random links near unity: each link is one RST proposal matrix (the
@@ -951,5 +957,172 @@ void launch_max_unitarity_dev(const Geom &g, const LinkField<T> &L, double *out,
 GLAC_INST(double)
 GLAC_INST(float)
 #undef GLAC_INST
+
+// ---------------------------------------------------------------------------
+// Batched ensemble (see LatSlot in kernels.cuh)
+// ---------------------------------------------------------------------------
+// Lattice of block b: the last i with start[i] <= b.
+__device__ __forceinline__ int slot_of(const int *__restrict__ start, int M, int b) {
+    int lo = 0, hi = M;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(start + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+ObsPlan make_obs_plan_capped(const Geom &g, int max_threads) {
+    const int half_slice = g.N[0] * g.N[1] * g.N[2] / 2;
+    int best = -1, best_score = 1 << 30;
+    for (int B = 1; B <= max_threads && B <= half_slice; B++) {
+        if (half_slice % B) continue;
+        const int score = (B % 32 == 0 ? 0 : 100000) + std::abs(B - max_threads);
+        if (score < best_score) { best_score = score; best = B; }
+    }
+    ObsPlan pl;
+    pl.Bv = best;
+    pl.B = (best + 31) / 32 * 32;
+    pl.nb = half_slice / best;
+    pl.nblocks = g.N[3] * 2 * pl.nb;
+    return pl;
+}
+
+int ens_blocks(const Geom &g, const ObsPlan &plan, int phase) {
+    switch (phase) {
+    case ENS_METRO: return (g.Vh + 127) / 128;
+    case ENS_FLOW0: return 8 * ((g.Vh + 127) / 128);
+    case ENS_FLOW1: return (g.Vh + 15) / 16;
+    default: return plan.nblocks;
+    }
+}
+
+// grid (sum of ENS_METRO blocks, 8 planes)
+template <typename T>
+__global__ void __launch_bounds__(128) kb_haar(const LatSlot<T> *__restrict__ slots, const int *__restrict__ start,
+                                               int M, uint32_t k0, uint32_t k1) {
+    const int i = slot_of(start, M, blockIdx.x);
+    const LatSlot<T> &S = slots[i];
+    const int s = (blockIdx.x - __ldg(start + i)) * 128 + threadIdx.x;
+    if (s >= S.g.Vh) return;
+    haar_link(S.g, S.f[0], blockIdx.y >> 1, blockIdx.y & 1, s, k0, k1, S.stream);
+}
+template <typename T>
+void launch_ens_haar(const LatSlot<T> *slots, const int *start, int nblocks, int M, uint64_t seed, cudaStream_t st) {
+    kb_haar<T><<<dim3(nblocks, 8), 128, 0, st>>>(slots, start, M, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+#define GLAC_ENS_METRO_KERNEL(NAME, ATTR)                                                                    \
+    template <typename T>                                                                                  \
+    __global__ void ATTR NAME(const LatSlot<T> *__restrict__ slots, const int *__restrict__ start, int M,    \
+                              int fsel, int mu, int p, T eps, T sq1me, int nhits, uint32_t k0, uint32_t k1,  \
+                              const uint32_t *__restrict__ sweep_base, uint32_t sweep_off, bool flips) {     \
+        const int i = slot_of(start, M, blockIdx.x);                                                       \
+        const LatSlot<T> &S = slots[i];                                                                    \
+        Proposal P;                                                                                        \
+        P.flips = flips;                                                                                   \
+        metropolis_body<T, false>(S.g, S.f[fsel], mu, p, (T)(-S.beta / 3.f), eps, sq1me, nhits, k0, k1,     \
+                                  __ldg(sweep_base) + sweep_off, S.stream, S.acc, P, S.beta,               \
+                                  blockIdx.x - __ldg(start + i));                                          \
+    }
+GLAC_ENS_METRO_KERNEL(kb_metropolis, __launch_bounds__(128))
+GLAC_ENS_METRO_KERNEL(kb_metropolis_r128, __maxnreg__(128))
+GLAC_ENS_METRO_KERNEL(kb_metropolis_r96, __maxnreg__(96))
+GLAC_ENS_METRO_KERNEL(kb_metropolis_r80, __maxnreg__(80))
+#undef GLAC_ENS_METRO_KERNEL
+
+template <typename T>
+void launch_ens_metropolis(const LatSlot<T> *slots, const int *start, int nblocks, int M, int fsel, int mu, int p,
+                           double eps, int nhits, uint64_t seed, const uint32_t *sweep_base, uint32_t sweep_off,
+                           bool flips, int variant, cudaStream_t st) {
+    const T e = (T)eps, sq = (T)sqrt(1.0 - eps * eps);
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    switch (variant_regs(FAM_METRO, sizeof(T) == 4, variant)) {
+    case 128: kb_metropolis_r128<T><<<nblocks, 128, 0, st>>>(slots, start, M, fsel, mu, p, e, sq, nhits, k0, k1, sweep_base, sweep_off, flips); break;
+    case 96: kb_metropolis_r96<T><<<nblocks, 128, 0, st>>>(slots, start, M, fsel, mu, p, e, sq, nhits, k0, k1, sweep_base, sweep_off, flips); break;
+    case 80: kb_metropolis_r80<T><<<nblocks, 128, 0, st>>>(slots, start, M, fsel, mu, p, e, sq, nhits, k0, k1, sweep_base, sweep_off, flips); break;
+    default: kb_metropolis<T><<<nblocks, 128, 0, st>>>(slots, start, M, fsel, mu, p, e, sq, nhits, k0, k1, sweep_base, sweep_off, flips); break;
+    }
+}
+
+#define GLAC_ENS_FLOW_KERNEL(NAME, ATTR)                                                                     \
+    template <typename T, int STAGE, int SHAPE>                                                            \
+    __global__ void ATTR NAME(const LatSlot<T> *__restrict__ slots, const int *__restrict__ start, int M,    \
+                              int src, int dst, T alpha, T beta) {                                         \
+        const int i = slot_of(start, M, blockIdx.x);                                                       \
+        const LatSlot<T> &S = slots[i];                                                                    \
+        flow_stage_body<T, EXP_MORNINGSTAR, STAGE, SHAPE>(S.g, S.f[src], S.f[dst], S.z, alpha, beta,         \
+                                                          blockIdx.x - __ldg(start + i));                  \
+    }
+GLAC_ENS_FLOW_KERNEL(kb_flow_stage, __launch_bounds__(128))
+GLAC_ENS_FLOW_KERNEL(kb_flow_stage_r80, __maxnreg__(80))
+GLAC_ENS_FLOW_KERNEL(kb_flow_stage_r128, __maxnreg__(128))
+#undef GLAC_ENS_FLOW_KERNEL
+
+template <typename T, int STAGE>
+static void ens_flow_dispatch(int regs, int shape, int nblocks, cudaStream_t st, const LatSlot<T> *slots,
+                              const int *start, int M, int src, int dst, T a, T b) {
+    if (shape == 1) {
+        kb_flow_stage<T, STAGE, 1><<<nblocks, 128, 0, st>>>(slots, start, M, src, dst, a, b);
+        return;
+    }
+    switch (regs) {
+    case 128: kb_flow_stage_r128<T, STAGE, 0><<<nblocks, 128, 0, st>>>(slots, start, M, src, dst, a, b); break;
+    case 80:
+        if constexpr (sizeof(T) == 4) {
+            kb_flow_stage_r80<T, STAGE, 0><<<nblocks, 128, 0, st>>>(slots, start, M, src, dst, a, b);
+            break;
+        }
+        [[fallthrough]];
+    default: kb_flow_stage<T, STAGE, 0><<<nblocks, 128, 0, st>>>(slots, start, M, src, dst, a, b); break;
+    }
+}
+
+// nblocks: the table of the variant's shape (ENS_FLOW0 or ENS_FLOW1)
+template <typename T>
+void launch_ens_flow_stage(const LatSlot<T> *slots, const int *start, int nblocks, int M, int src, int dst, int stage,
+                           double alpha, double beta, int variant, cudaStream_t st) {
+    const bool fp32 = sizeof(T) == 4;
+    const int regs = variant_regs(FAM_FLOW, fp32, variant), shape = variant_shape(FAM_FLOW, fp32, variant);
+    const T a = (T)alpha, b = (T)beta;
+    if (stage == 0) ens_flow_dispatch<T, 0>(regs, shape, nblocks, st, slots, start, M, src, dst, a, b);
+    else if (stage == 1) ens_flow_dispatch<T, 1>(regs, shape, nblocks, st, slots, start, M, src, dst, a, b);
+    else ens_flow_dispatch<T, 2>(regs, shape, nblocks, st, slots, start, M, src, dst, a, b);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) kb_observables(const LatSlot<T> *__restrict__ slots,
+                                                      const int *__restrict__ start, int M, int fsel) {
+    const int i = slot_of(start, M, blockIdx.x);
+    const LatSlot<T> &S = slots[i];
+    observables_body<T>(S.g, S.f[fsel], S.nb, S.Bv, S.partial, blockIdx.x - __ldg(start + i));
+}
+template <typename T>
+__global__ void kb_obs_finalize(const LatSlot<T> *__restrict__ slots, int meas) {
+    const LatSlot<T> &S = slots[blockIdx.x];
+    obs_finalize_body(S.g.N[3], S.nb, S.g.V, S.partial, S.obs + (size_t)meas * (3 + S.g.N[3]));
+}
+template <typename T>
+void launch_ens_observables(const LatSlot<T> *slots, const int *start, int nblocks, int M, int fsel, int meas,
+                            int variant, cudaStream_t st) {
+    (void)variant;
+    kb_observables<T><<<nblocks, 128, 0, st>>>(slots, start, M, fsel);
+    kb_obs_finalize<T><<<M, 256, 0, st>>>(slots, meas);
+}
+
+__global__ void k_advance(uint32_t *counter, uint32_t by) { counter[0] += by; }
+void launch_advance(uint32_t *counter, uint32_t by, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(counter, by); }
+
+#define GLAC_ENS_INST(T)                                                                                      \
+    template void launch_ens_haar<T>(const LatSlot<T> *, const int *, int, int, uint64_t, cudaStream_t);      \
+    template void launch_ens_metropolis<T>(const LatSlot<T> *, const int *, int, int, int, int, int, double,  \
+                                           int, uint64_t, const uint32_t *, uint32_t, bool, int, cudaStream_t); \
+    template void launch_ens_flow_stage<T>(const LatSlot<T> *, const int *, int, int, int, int, int, double,  \
+                                           double, int, cudaStream_t);                                        \
+    template void launch_ens_observables<T>(const LatSlot<T> *, const int *, int, int, int, int, int,         \
+                                            cudaStream_t);
+GLAC_ENS_INST(double)
+GLAC_ENS_INST(float)
+#undef GLAC_ENS_INST
 
 }  // namespace glac

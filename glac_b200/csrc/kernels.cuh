@@ -109,4 +109,39 @@ void launch_delta_s(double beta, long n, const double *U, const double *Up, cons
 template <typename T>
 void launch_max_unitarity_dev(const Geom &g, const LinkField<T> &L, double *out, cudaStream_t st);
 
+// ---------------------------------------------------------------------------
+// Batched ensemble: many independent lattices per launch.  Each phase kernel
+// walks a prefix table of block counts (start[i] = first block of lattice i,
+// start[M] = total) and runs the single-lattice body on lattice i's slot.
+// ---------------------------------------------------------------------------
+template <typename T> struct LatSlot {
+    Geom g;
+    LinkField<T> f[3];        // 0: Markov chain, 1 and 2: flow ping-pong
+    ForceField<T> z;
+    int nb, Bv;               // observable plan (blocks of <= 128 threads)
+    double *partial;          // 3 doubles per observable block
+    double *obs;              // this lattice's measurement rows (3 + Nt each)
+    unsigned long long *acc;  // accepted proposals
+    float beta;
+    uint32_t stream;          // Philox stream
+};
+enum EnsPhase { ENS_METRO = 0, ENS_FLOW0 = 1, ENS_FLOW1 = 2, ENS_OBS = 3, ENS_NPHASE = 4 };
+// blocks of one lattice per phase (FLOW0/FLOW1: flow site-block shape 0/1)
+int ens_blocks(const Geom &g, const ObsPlan &plan, int phase);
+ObsPlan make_obs_plan_capped(const Geom &g, int max_threads);
+
+template <typename T>
+void launch_ens_haar(const LatSlot<T> *slots, const int *start, int nblocks, int M, uint64_t seed, cudaStream_t st);
+template <typename T>
+void launch_ens_metropolis(const LatSlot<T> *slots, const int *start, int nblocks, int M, int fsel, int mu, int p,
+                           double eps, int nhits, uint64_t seed, const uint32_t *sweep_base, uint32_t sweep_off,
+                           bool flips, int variant, cudaStream_t st);
+template <typename T>
+void launch_ens_flow_stage(const LatSlot<T> *slots, const int *start, int nblocks, int M, int src, int dst, int stage,
+                           double alpha, double beta, int variant, cudaStream_t st);
+template <typename T>
+void launch_ens_observables(const LatSlot<T> *slots, const int *start, int nblocks, int M, int fsel,
+                            int meas, int variant, cudaStream_t st);
+void launch_advance(uint32_t *counter, uint32_t by, cudaStream_t st);
+
 }  // namespace glac

@@ -201,12 +201,13 @@ def train_proposal(feat, esj, grid=DEFAULT_GRID, steps=3000, batch=8192, lr=2e-3
 
 
 def run_chain(start, dims, beta, precision, sweeps, meas_every, flow_eps, flow_steps, seed, params=None,
-              grid=DEFAULT_GRID, su3_eps=0.24, flips=True, label=""):
+              grid=DEFAULT_GRID, su3_eps=0.24, flips=True, label="", reunit_interval=10):
     """One chain from `start`: plaquette after every sweep, Q(t = flow_eps * flow_steps) every meas_every."""
     plaq = np.empty(sweeps)
     Q = []
     acc = 0.0
-    with Lattice(dims, beta=beta, precision=precision, su3_eps=su3_eps, seed=seed) as L, \
+    reunit = reunit_interval if precision == "fp32" else 0
+    with Lattice(dims, beta=beta, precision=precision, su3_eps=su3_eps, seed=seed, reunit_interval=reunit) as L, \
             Lattice(dims, beta=beta, precision=precision, flow_eps=flow_eps, seed=seed) as F:
         L.set_links(start)
         L.set_option("su2_sign_flips", int(flips))
@@ -226,11 +227,13 @@ def run_chain(start, dims, beta, precision, sweeps, meas_every, flow_eps, flow_s
                 Q.append(F.measure()[1])
         F.sync()
         wall = time.perf_counter() - t0
+        unitarity = L.unitarity_violation()
     Q = np.asarray(Q)
     gp, gq = gamma_method(plaq), gamma_method(Q)
     return dict(
         label=label, precision=precision, learned=params is not None, su3_eps=None if params is not None else su3_eps,
         su2_sign_flips=bool(flips), sweeps=sweeps, wall_s=wall, acceptance=acc / sweeps,
+        reunit_interval=reunit, unitarity_violation_end=unitarity,
         plaquette=gp.mean, plaquette_err=gp.error, tau_int_plaquette=gp.tau_int, tau_int_plaquette_err=gp.tau_error,
         n_Q=int(Q.size), Q2=float(np.mean(Q * Q)), Q2_err=float(gamma_method(Q * Q).error),
         tau_int_Q=gq.tau_int * meas_every, tau_int_Q_err=gq.tau_error * meas_every,
@@ -246,10 +249,11 @@ def tau_study(dims=(24, 24, 24, 48), beta=6.0, therm=500, train_sweeps=2000, eve
                esj_stride=stride, esj_trials=trials, sweeps=sweeps, meas_every=meas_every, flow_eps=flow_eps,
                flow_t=flow_t, grid=[float(x) for x in DEFAULT_GRID])
     t0 = time.time()
-    with Lattice(dims, beta=beta, precision="fp32", seed=seed) as L:
+    with Lattice(dims, beta=beta, precision="fp32", seed=seed, reunit_interval=10) as L:
         L.hot_start(seed)
         L.metropolis(therm)
         feat, esj, plain = collect_esj(L, train_sweeps, every, stride, DEFAULT_GRID, trials)
+        L.reunitarize()
         start = L.get_links()
     out["collect_seconds"] = time.time() - t0
     net, rep = train_proposal(feat, esj, DEFAULT_GRID, steps=steps, seed=seed, esj_plain=plain)

@@ -234,6 +234,51 @@ glac_status glac_mlp_loss_grad(glac_mlp *mlp, const float *dev_features, const f
 glac_status glac_mlp_train(glac_mlp *mlp, const float *dev_features, const float *dev_esj, long long n, int n_eps,
                            const double *eps_grid, int steps, long long batch, double lr, double *host_losses);
 
+/* ---- batched ensemble (no counterpart in the reference) ----------------- */
+/* Many independent lattices of uneven sizes and couplings driven together: each
+ * Metropolis sub-sweep, flow stage and observable pass is one launch over all
+ * of them, and glac_ensemble_run replays the whole schedule as one CUDA graph.
+ * Lattice i is dims[4i .. 4i+3] at coupling betas[i]; `common` supplies the
+ * precision, n_updates, su3_eps, flow_eps, exp_func (Morningstar only), the
+ * Philox key `seed`, the first stream id (lattice i uses stream_id + i, so it
+ * draws exactly what a single context with that stream id draws) and the device;
+ * common->dims and beta are ignored. */
+typedef struct glac_ensemble glac_ensemble;
+glac_status glac_ensemble_create(int n, const int *dims, const double *betas, const glac_desc *common,
+                                 glac_ensemble **out);
+void glac_ensemble_destroy(glac_ensemble *ens);
+const char *glac_ensemble_last_error(const glac_ensemble *ens);
+/* Message of the last failed glac_ensemble_create on this thread. */
+const char *glac_ensemble_global_error(void);
+uint64_t glac_ensemble_launch_count(const glac_ensemble *ens);
+/* "su2_sign_flips" 0/1 as for glac_set_option. */
+glac_status glac_ensemble_set_option(glac_ensemble *ens, const char *key, long value);
+/* Seeded Haar start of every lattice (as glac_hot_start with the lattice's stream). */
+glac_status glac_ensemble_hot_start(glac_ensemble *ens, uint64_t seed);
+/* Lattice i's Markov-chain field in the host layout of glac_set_links. */
+glac_status glac_ensemble_set_links(glac_ensemble *ens, int i, const double *host_links);
+glac_status glac_ensemble_get_links(glac_ensemble *ens, int i, double *host_links);
+/* n checkerboard sweeps of every lattice; acceptance[i] (may be NULL) per lattice. */
+glac_status glac_ensemble_metropolis(glac_ensemble *ens, int n_sweeps, double *acceptance);
+/* Doubles of the measurement output for n_steps flow steps: lattice i holds
+ * (n_steps + 1) rows of 3 + Nt_i (plaq, topc, energy, topct), lattices in order. */
+long long glac_ensemble_obs_count(const glac_ensemble *ens, int n_steps);
+/* Flow copies of every chain field (System::flowConfiguration, GLAC/system.cpp:
+ * 471-517): measurement at t = 0 and after each of n_steps RK3 steps; the
+ * chains are not modified.  obs (may be NULL): glac_ensemble_obs_count doubles. */
+glac_status glac_ensemble_flow(glac_ensemble *ens, int n_steps, double *obs);
+/* n_sweeps sweeps then the flow of glac_ensemble_flow, as one CUDA graph launch
+ * (captured on the first call for this (n_sweeps, n_steps), replayed after);
+ * gpu_seconds (may be NULL) = device time of the graph. */
+glac_status glac_ensemble_run(glac_ensemble *ens, int n_sweeps, int n_steps, double *acceptance, double *obs,
+                              double *gpu_seconds);
+/* Launch-variant autotuner over the whole ensemble (flow site-block shapes and
+ * register caps, Metropolis register caps); report[4 f + v] = seconds per
+ * flow step (f = 0) / per sweep (f = 1) of variant v.  Leaves the chains as they were. */
+glac_status glac_ensemble_autotune(glac_ensemble *ens, int reps, double *report);
+glac_status glac_ensemble_get_tuning(const glac_ensemble *ens, int *variants3);
+glac_status glac_ensemble_set_tuning(glac_ensemble *ens, const int *variants3);
+
 /* ---- gauge-field files (GLAC/io/fieldio.cpp) ----------------------------- */
 /* Read a GLAC .bin configuration (per site 4 links x 18 doubles, x fastest;
  * fieldio.cpp:195-257) or, with chroma != 0, its byte-swapped Chroma variant

@@ -95,3 +95,12 @@ def test_field_io_errors(tmp_path):
     with pytest.raises(g.GlacError) as e:
         g.read_field(str(short), (4, 4, 4, 4))
     assert e.value.status == g.GLAC_ERR_IO and "expected" in str(e.value)
+
+
+def test_ensemble_draw_is_seeded_and_uneven():
+    from glac_b200.ensemble import BETAS, SIZES, draw_ensemble
+    d1, b1 = draw_ensemble(20261203, 64)
+    d2, b2 = draw_ensemble(20261203, 64)
+    assert d1 == d2 and b1 == b2 and len(d1) == 64
+    assert set(d1) <= set(SIZES) and set(b1) <= set(BETAS)
+    assert len(set(d1)) == 4 and len(set(b1)) == 4  # every size and coupling occurs
