@@ -284,6 +284,20 @@ def run_gpu(args):
     torch.cuda.synchronize()
     t64 = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
     rate64 = world * V * k64 / t64
+    # plain FP64 Metropolis (the reference's proposal at su3_eps) on the same field
+    L64m = g.Lattice(DIMS, beta=BETA, precision="fp64", n_updates=NHITS, su3_eps=SU3_EPS, seed=20261203,
+                     stream_id=rank, device=local)
+    L64m.set_links(start)
+    s64m = torch.cuda.ExternalStream(L64m.stream)
+    L64m.metropolis(2)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0.record(s64m)
+    L64m.metropolis(10)
+    e1.record(s64m)
+    torch.cuda.synchronize()
+    metro64_rate = world * 4 * V * 10 / max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+    L64m.close()
     L64.close()
 
     # end to end through the C ABI: pinned host field in, host observables out
@@ -300,6 +314,45 @@ def run_gpu(args):
            "how": "glac_flow_configuration: H2D of the FP64 host field, K steps with per-step observables, D2H"}
     obs_last = obs_e2e.numpy().reshape(args.steps + 1, -1)[-1]
 
+    # learned proposal spread on this lattice: ESJ data from 100 plain sweeps,
+    # training on the GPU, then the learned sampler's link-updates/s
+    learned_extra = None
+    if not args.no_learned:
+        from glac_b200 import learned as lp
+        feat, esj, plain = lp.collect_esj(L, 100, 10, 64, lp.DEFAULT_GRID, trials=4)
+        net, rep = lp.train_proposal(feat, esj, lp.DEFAULT_GRID, steps=1000, batch=8192, lr=2e-3, seed=1,
+                                     esj_plain=plain)
+        params = net.params
+        net.close()
+        del feat, esj, plain
+        L.set_option("su2_sign_flips", 0)
+        L.set_proposal_net(params, float(lp.DEFAULT_GRID[0]), float(lp.DEFAULT_GRID[-1]))
+        L.metropolis(2)
+        t_l = timed(lambda: L.metropolis(1), 20)
+        L.set_proposal_net(None)
+        L.set_option("su2_sign_flips", 1)
+        learned_extra = {"metropolis_link_updates_per_s_fp32_learned": world * 4 * V * 20 / t_l,
+                         "esj_per_link_update_learned": rep["esj_learned"],
+                         "esj_per_link_update_plain": rep["esj_plain_reference_proposal"],
+                         "esj_gain_learned_vs_plain": rep["gain_vs_plain"],
+                         "esj_gain_learned_vs_best_fixed_spread": rep["gain_vs_best_fixed"],
+                         "training_rows": rep["rows_train"], "training_seconds": rep["train_seconds"]}
+
+    # batched ensemble: 64 seeded uneven lattices, 100 sweeps + 200 flow steps as one CUDA graph
+    ens_extra = None
+    if not args.no_ensemble and world == 1:
+        from glac_b200 import ensemble as en
+        dims_l, betas_l = en.draw_ensemble(20261203, 64)
+        with en.Ensemble(dims_l, betas_l, precision="fp32", seed=20261203) as E:
+            E.hot_start(20261203)
+            tune_e = E.autotune(2)
+            E.run(100, 200)  # capture
+            _, obs_e, sec_e = E.run(100, 200)
+        sites_e = int(sum(np.prod(d) for d in dims_l))
+        ens_extra = {"lattices": 64, "sites": sites_e, "graph_gpu_s": sec_e,
+                     "link_updates_plus_flow_site_steps_per_s": sites_e * (4 * 100 + 200) / sec_e,
+                     "autotune_chosen": tune_e["chosen"], "plaq_after_flow_mean": float(np.mean([o[-1, 0] for o in obs_e]))}
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_main / args.steps * 1e3, "higher_is_better": True,
@@ -315,6 +368,9 @@ def run_gpu(args):
             "flow_site_steps_per_s_no_obs": rate_noobs,
             "flow_site_steps_per_s_fp64_with_obs": rate64,
             "metropolis_link_updates_per_s_fp32": metro_rate,
+            "metropolis_link_updates_per_s_fp64": metro64_rate,
+            "learned": learned_extra,
+            "ensemble_64_uneven": ens_extra,
             "metropolis_acceptance": acc_holder.get("a"),
             "plaq_after_flow": float(obs_last[0]),
             "autotune": tuned,
@@ -403,6 +459,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=25)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-lattice ensemble leg")
     ap.add_argument("--profile", choices=["flow", "metropolis"], help="small workload for ncu / variant timing")
     ap.add_argument("--dims", default="32,32,32,64")
     ap.add_argument("--precision", default="fp32")
