@@ -422,11 +422,31 @@ def run_profile(args):
     import torch
     import glac_b200 as g
     dims = tuple(int(x) for x in args.dims.split(","))
+    if args.profile == "ensemble":
+        # the seeded uneven ensemble, args.steps sweeps + args.steps flow steps eagerly
+        from glac_b200 import ensemble as en
+        dl, bl = en.draw_ensemble(20261203, args.ensemble_n)
+        with en.Ensemble(dl, bl, precision=args.precision, seed=5) as E:
+            E.hot_start(7)
+            if args.tune:
+                E.tuning = [int(x) for x in args.tune.split(",")]
+            E.metropolis(args.steps)
+            E.flow(args.steps)
+        return
     L = g.Lattice(dims, beta=BETA, precision=args.precision, flow_eps=FLOW_EPS, seed=5, device=0)
     L.hot_start(7)
     if args.tune:
         L.tuning = [int(x) for x in args.tune.split(",")]
-    if args.profile == "metropolis":
+    if args.profile == "learned":
+        # the learned sampler with a fixed random network (spread varying per link)
+        rng = np.random.default_rng(6)
+        P = np.zeros(g.MLP_NPARAMS, np.float32)
+        P[:256] = rng.standard_normal(256) * 0.5
+        P[288:1312] = rng.standard_normal(1024) * 0.25
+        P[1344:1376] = rng.standard_normal(32) * 0.3
+        L.set_option("su2_sign_flips", 0)
+        L.set_proposal_net(P, 0.1, 0.6)
+    if args.profile in ("metropolis", "learned"):
         L.metropolis(args.steps)
     else:
         L.flow(args.steps, measure=not args.no_obs)
@@ -436,7 +456,7 @@ def run_profile(args):
         st = torch.cuda.ExternalStream(L.stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
-        if args.profile == "metropolis":
+        if args.profile in ("metropolis", "learned"):
             L.metropolis(args.time_reps)
         else:
             L.flow(args.time_reps, measure=not args.no_obs)
@@ -446,7 +466,7 @@ def run_profile(args):
         stages = L.flow_stage_times(5) if args.profile == "flow" else None
         print(json.dumps({"profile": args.profile, "dims": dims, "precision": args.precision, "tune": L.tuning,
                           "ms_per_step": sec * 1e3,
-                          "rate": (4 * V if args.profile == "metropolis" else V) / sec,
+                          "rate": (4 * V if args.profile in ("metropolis", "learned") else V) / sec,
                           "stage_ms": None if stages is None else [x * 1e3 for x in stages]}))
     L.close()
 
@@ -461,7 +481,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-lattice ensemble leg")
-    ap.add_argument("--profile", choices=["flow", "metropolis"], help="small workload for ncu / variant timing")
+    ap.add_argument("--profile", choices=["flow", "metropolis", "learned", "ensemble"],
+                    help="small workload for ncu / variant timing")
+    ap.add_argument("--ensemble-n", type=int, default=16, help="lattices in the ensemble profile")
     ap.add_argument("--dims", default="32,32,32,64")
     ap.add_argument("--precision", default="fp32")
     ap.add_argument("--no-obs", action="store_true")
