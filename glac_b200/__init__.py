@@ -114,6 +114,9 @@ def lib() -> C.CDLL:
     L.glac_write_field.argtypes = [C.c_char_p, C.c_int * 4, _dp]
     # learned proposal spread
     L.glac_copy_field.argtypes = [P, P]
+    L.glac_measure_density.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.glac_get_sweep.argtypes = [P, C.POINTER(C.c_uint32)]
+    L.glac_set_sweep.argtypes = [P, C.c_uint32]
     L.glac_set_proposal_net.argtypes = [P, C.c_void_p, C.c_double, C.c_double]
     L.glac_esj_data.argtypes = [P, C.c_int, _dp, C.c_int, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_longlong, C.POINTER(C.c_longlong)]
@@ -324,6 +327,24 @@ class Lattice:
         self._ck(lib().glac_esj_data(self._ctx, g.size, g, int(trials), int(stride), int(snapshot), feat_ptr,
                                      esj_ptr if g.size else None, ids_ptr, int(capacity), C.byref(n)))
         return n.value
+
+    def measure_density(self):
+        """(observables, q density, e density): per-site fields of length V in the host site order."""
+        obs = np.empty(3 + self.Nt)
+        q, e = np.empty(self.V), np.empty(self.V)
+        self._ck(lib().glac_measure_density(self._ctx, obs.ctypes.data, q.ctypes.data, e.ctypes.data))
+        return obs, q, e
+
+    @property
+    def sweep(self) -> int:
+        """Philox sweep counter (advanced by every Metropolis sweep)."""
+        v = C.c_uint32(0)
+        self._ck(lib().glac_get_sweep(self._ctx, C.byref(v)))
+        return v.value
+
+    @sweep.setter
+    def sweep(self, v: int):
+        self._ck(lib().glac_set_sweep(self._ctx, int(v)))
 
     def copy_from(self, other: "Lattice"):
         """Device copy of another context's field (same dimensions and precision)."""

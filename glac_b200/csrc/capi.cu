@@ -431,6 +431,44 @@ glac_status glac_measure(glac_ctx *c, double *obs) {
     });
 }
 
+glac_status glac_measure_density(glac_ctx *c, double *obs, double *q_density, double *e_density) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        if (!q_density || !e_density) {
+            c->err = "null density output";
+            return GLAC_ERR_ARG;
+        }
+        const size_t n = 3 + (size_t)c->g.N[3], V = (size_t)c->g.V;
+        ensure_obs(c, n);
+        ensure_staging(c);  // V * 72 doubles: room for both densities
+        double *dq = c->staging, *de = c->staging + V;
+        if (c->d.precision == GLAC_FP64)
+            launch_observables_density(c->g, f64(c, c->cur), c->plan, c->partial, c->obs_dev, dq, de, c->stream);
+        else
+            launch_observables_density(c->g, f32(c, c->cur), c->plan, c->partial, c->obs_dev, dq, de, c->stream);
+        ck_launch("observables density");
+        c->launches += 2;
+        if (obs) ck(cudaMemcpyAsync(obs, c->obs_dev, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaMemcpyAsync(q_density, dq, V * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H q");
+        ck(cudaMemcpyAsync(e_density, de, V * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H e");
+        ck(cudaStreamSynchronize(c->stream), "sync");
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_get_sweep(glac_ctx *c, uint32_t *sweep) {
+    if (!c || !sweep) return GLAC_ERR_ARG;
+    *sweep = c->sweep;
+    return GLAC_OK;
+}
+
+glac_status glac_set_sweep(glac_ctx *c, uint32_t sweep) {
+    if (!c) return GLAC_ERR_ARG;
+    c->sweep = sweep;
+    return GLAC_OK;
+}
+
 glac_status glac_flow(glac_ctx *c, int n_steps, double *obs) {
     return guarded(c, [&] {
         glac_status s = need_field(c);

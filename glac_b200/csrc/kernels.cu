@@ -525,9 +525,13 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
+// With dq/de set, also the per-site densities in lexicographic order:
+// dq[n] = -(1/(16^2 pi^2)) sum ReTr(C_0nu C_rhosigma), de[n] = sum ReTr(C C) (unnormalised),
+// the fields LatticeActionChargeDensity writes (latticeactionchargedensity.cpp:169-306).
 template <typename T>
 __device__ __forceinline__ void observables_body(const Geom &g, const LinkField<T> &L, int nb, int Bv,
-                                                 double *partial, int b) {
+                                                 double *partial, int b, double *dq = nullptr,
+                                                 double *de = nullptr) {
     const int t = b / (2 * nb);
     const int p = (b / nb) & 1;
     const int j = b % nb;
@@ -546,6 +550,10 @@ __device__ __forceinline__ void observables_body(const Geom &g, const LinkField<
             plaq += (double)pl1 + (double)pl2;
             qt -= (double)retr_ah(F1, F2);
             en += (double)retr_ah(F1, F1) + (double)retr_ah(F2, F2);
+        }
+        if (dq) {
+            dq[n.lex] = qt * (1.0 / (16 * 16 * M_PI * M_PI));
+            de[n.lex] = en;
         }
     }
     // deterministic block reduction
@@ -616,6 +624,22 @@ void launch_observables(const Geom &g, const LinkField<T> &L, const ObsPlan &pla
     }
     k_obs_finalize<<<1, 256, 0, st>>>(g.N[3], plan.nb, g.V, partial, out);
 }
+template <typename T>
+__global__ void __launch_bounds__(256) k_observables_density(Geom g, LinkField<T> L, int nb, int Bv, double *partial,
+                                                             double *dq, double *de) {
+    observables_body<T>(g, L, nb, Bv, partial, blockIdx.x, dq, de);
+}
+template <typename T>
+void launch_observables_density(const Geom &g, const LinkField<T> &L, const ObsPlan &plan, double *partial,
+                                double *out, double *dq, double *de, cudaStream_t st) {
+    if (g.N[3] > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
+    k_observables_density<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial, dq, de);
+    k_obs_finalize<<<1, 256, 0, st>>>(g.N[3], plan.nb, g.V, partial, out);
+}
+template void launch_observables_density<double>(const Geom &, const LinkField<double> &, const ObsPlan &, double *,
+                                                 double *, double *, double *, cudaStream_t);
+template void launch_observables_density<float>(const Geom &, const LinkField<float> &, const ObsPlan &, double *,
+                                                double *, double *, double *, cudaStream_t);
 template void launch_observables<double>(const Geom &, const LinkField<double> &, const ObsPlan &, double *,
                                          double *, int, cudaStream_t);
 template void launch_observables<float>(const Geom &, const LinkField<float> &, const ObsPlan &, double *,

@@ -133,20 +133,23 @@ void ObservableStorer::run_statistics() {
 
 // GLAC/system.cpp:62-125
 Sampler select_sampler(const std::vector<std::string> &names) {
-    bool plaq = false, topc = false, energy = false, topct = false;
+    bool plaq = false, topc = false, energy = false, topct = false, density = false;
     for (const std::string &n : names) {
         if (n == "plaq") plaq = true;
         else if (n == "topc") topc = true;
         else if (n == "energy") energy = true;
         else if (n == "topct") topct = true;
+        else if (n == "energyTopcFieldDensity") density = true;
         else throw std::runtime_error("observable \"" + n + "\" is not provided by this implementation");
     }
     if ((topc || energy) && !topct) return Sampler::Master;
     if (plaq && !topc && !energy && !topct) return Sampler::Plaquette;
+    if (density && !plaq && !topc && !energy && !topct) return Sampler::ChargeDensity;
     return Sampler::MasterTopcXYZ;
 }
 std::vector<std::string> sampler_names(Sampler s, bool flow) {
     if (s == Sampler::Plaquette) return {"plaq"};
+    if (s == Sampler::ChargeDensity) return {"plaq", "topc", "energy"};
     if (s == Sampler::Master || !flow) return {"plaq", "topc", "energy"};
     return {"plaq", "topc", "energy", "topct"};
 }
@@ -169,6 +172,19 @@ static std::string cfg_number(const Parameters &P, unsigned n) {
 std::string fieldFileName(const Parameters &P, unsigned configNumber) {
     return P.batchName + "_b" + std::to_string(P.beta) + "_N" + std::to_string(P.NSpatial) + "_NT" +
            std::to_string(P.NTemporal) + "_np1_config" + cfg_number(P, configNumber) + ".bin";
+}
+
+void writeScalarField(const Parameters &P, const std::string &observable, const std::vector<double> &field,
+                      unsigned configNumber) {
+    const std::string dir = P.pwd + P.outputFolder + P.batchName + "/scalar_fields/" + observable + "/";
+    makeDirs(dir);
+    const std::string fname = dir + fieldFileName(P, configNumber);
+    std::FILE *f = std::fopen(fname.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot write " + fname);
+    const size_t n = std::fwrite(field.data(), sizeof(double), field.size(), f);
+    std::fclose(f);
+    if (n != field.size()) throw std::runtime_error("short write " + fname);
+    std::printf("\n    %s written.", fname.c_str());
 }
 
 // GLAC/io/observablesio.cpp:29-78
@@ -226,6 +242,24 @@ System::System(const Parameters &p) : P(p) {
     cfgSampler = select_sampler(P.observables);
     flowSampler = select_sampler(P.flowObservables);
     V = P.NSpatial * P.NSpatial * P.NSpatial * P.NTemporal;
+    if (cfgSampler == Sampler::ChargeDensity || flowSampler == Sampler::ChargeDensity) {
+        // one configuration, none stored, to keep the number of field files down (GLAC/system.cpp:105-113)
+        P.NCf = 1;
+        P.storeConfigurations = false;
+    }
+}
+
+void System::measureInto(glac_ctx *c, Sampler s, unsigned index, bool write, std::vector<double> &obs) {
+    obs.resize(3 + P.NTemporal);
+    if (s != Sampler::ChargeDensity || !write) {
+        if (glac_measure(c, obs.data()) != GLAC_OK) throw std::runtime_error(std::string("measure: ") + glac_last_error(c));
+        return;
+    }
+    std::vector<double> q(V), e(V);
+    if (glac_measure_density(c, obs.data(), q.data(), e.data()) != GLAC_OK)
+        throw std::runtime_error(std::string("measure density: ") + glac_last_error(c));
+    writeScalarField(P, "topc", q, index);
+    writeScalarField(P, "energy", e, index);
 }
 
 System::~System() {
@@ -298,7 +332,7 @@ void System::thermalize() {
     std::vector<double> obs(3 + P.NTemporal);
     if (P.storeThermalizationObservables) {
         NThermSteps = 1 + P.NTherm;
-        ck(glac_measure(ctx, obs.data()), "measure");
+        measureInto(ctx, cfgSampler, 0, true, obs);
         storeConfigObservables(0, obs);
     }
     double accept = 0.0;
@@ -311,7 +345,7 @@ void System::thermalize() {
         if (i % 20 == 0)
             std::printf("\n%6.2f %% done. Avg. update time: %10.6f sec", 100.0 * i / P.NTherm, updateSeconds / i);
         if (P.storeThermalizationObservables) {
-            ck(glac_measure(ctx, obs.data()), "measure");
+            measureInto(ctx, cfgSampler, i, true, obs);
             storeConfigObservables(i, obs);
         }
     }
@@ -337,7 +371,7 @@ void System::runMetropolis() {
             flowConfiguration(iConfig);  // flows a copy; the chain field stays in ctx
             obs = lastFlowT0;
         } else {
-            ck(glac_measure(ctx, obs.data()), "measure");
+            measureInto(ctx, cfgSampler, iConfig + NThermSteps, true, obs);
         }
         storeConfigObservables(iConfig + NThermSteps, obs);
         std::printf("\n%-4u %-20.8f %-12.8f", iConfig, obs[0], seconds / ((iConfig + 1) * (double)P.NCor));
@@ -378,8 +412,21 @@ void System::flowConfiguration(unsigned iConfig) {
     ck(glac_copy_field(flowCtx, ctx), "copy to flow lattice");
     const unsigned per = 3 + P.NTemporal;
     std::vector<double> obs((size_t)(P.NFlows + 1) * per);
-    glac_status st = glac_flow(flowCtx, (int)P.NFlows, obs.data());
-    if (st != GLAC_OK) throw std::runtime_error(std::string("flow: ") + glac_last_error(flowCtx));
+    if (flowSampler == Sampler::ChargeDensity) {
+        // step by step: the per-site fields every samplingFrequency flow steps
+        // (LatticeActionChargeDensity::calculate, :277-294; file number = flow step)
+        std::vector<double> o;
+        const unsigned sf = P.samplingFrequency > 0 ? (unsigned)P.samplingFrequency : 1u;
+        for (unsigned i = 0; i <= P.NFlows; i++) {
+            if (i > 0 && glac_flow(flowCtx, 1, nullptr) != GLAC_OK)
+                throw std::runtime_error(std::string("flow: ") + glac_last_error(flowCtx));
+            measureInto(flowCtx, flowSampler, i, i % sf == 0, o);
+            std::copy(o.begin(), o.end(), obs.begin() + (size_t)i * per);
+        }
+    } else {
+        glac_status st = glac_flow(flowCtx, (int)P.NFlows, obs.data());
+        if (st != GLAC_OK) throw std::runtime_error(std::string("flow: ") + glac_last_error(flowCtx));
+    }
     lastFlowT0.assign(obs.begin(), obs.begin() + per);
     if (P.verbose)
         for (unsigned i = 0; i < P.NFlows + 1; i++)
@@ -410,6 +457,20 @@ void System::load(const std::string &name) {
     if (st != GLAC_OK) throw std::runtime_error(glac_io_error());
     ck(glac_set_links(ctx, host.data()), "set links");
     std::printf("\nConfiguration %s loaded", path.c_str());
+    // random-stream checkpoint written beside stored configurations: continue the chain's stream
+    std::ifstream rng(path + ".rng");
+    std::string key;
+    double seed = 0;
+    unsigned sweep = 0;
+    if (rng >> key >> seed >> key >> sweep) {
+        if (seed == P.metropolisSeed) {
+            ck(glac_set_sweep(ctx, sweep), "set sweep");
+            std::printf("; random stream continues at sweep %u", sweep);
+        } else {
+            std::printf("; its random-stream checkpoint is for metropolisSeed %g, not %g: stream restarts", seed,
+                        P.metropolisSeed);
+        }
+    }
 }
 
 // GLAC/system.cpp:519-539
@@ -442,6 +503,11 @@ void System::writeFieldToFile(unsigned iConfig) {
     const int dims[4] = {(int)P.NSpatial, (int)P.NSpatial, (int)P.NSpatial, (int)P.NTemporal};
     const std::string fname = fieldFileName(P, iConfig);
     if (glac_write_field((dir + fname).c_str(), dims, host.data()) != GLAC_OK) throw std::runtime_error(glac_io_error());
+    // random-stream checkpoint (no counterpart in the reference): seed and Philox sweep counter
+    uint32_t sweep = 0;
+    ck(glac_get_sweep(ctx, &sweep), "get sweep");
+    std::ofstream rng(dir + fname + ".rng");
+    rng << "metropolisSeed " << std::setprecision(17) << P.metropolisSeed << "\nsweep " << sweep << "\n";
     std::printf("    %s written.", fname.c_str());
 }
 

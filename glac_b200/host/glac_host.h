@@ -62,8 +62,10 @@ struct ObservableStorer {
 };
 
 // Which observables a list selects (GLAC/system.cpp:62-125): plaquette only, the
-// three-observable MasterSampler, or MasterSamplerTopcXYZ (adds topct).
-enum class Sampler { Plaquette, Master, MasterTopcXYZ };
+// three-observable MasterSampler, MasterSamplerTopcXYZ (adds topct), or
+// LatticeActionChargeDensity (energyTopcFieldDensity alone: per-site q and E
+// fields written to scalar_fields/).
+enum class Sampler { Plaquette, Master, MasterTopcXYZ, ChargeDensity };
 Sampler select_sampler(const std::vector<std::string> &names);
 std::vector<std::string> sampler_names(Sampler s, bool flow);
 
@@ -85,6 +87,9 @@ private:
     void writeFieldToFile(unsigned iConfig);
     void storeConfigObservables(unsigned index, const std::vector<double> &obs);
     void checkLattice(const std::string &where);
+    // glac_measure, or for the charge-density sampler also the per-site fields,
+    // written when `write` (LatticeActionChargeDensity::calculate, :277-305)
+    void measureInto(glac_ctx *c, Sampler s, unsigned index, bool write, std::vector<double> &obs);
     void ck(glac_status s, const char *what);
     std::string outDir() const;
 
@@ -108,6 +113,9 @@ void writeFlowObservableToFile(const Parameters &P, const std::string &name, con
 void writeMatrixToFile(const Parameters &P, const std::string &name, const std::vector<double> &values,
                        unsigned configNumber, unsigned N);
 std::string fieldFileName(const Parameters &P, unsigned configNumber);
+// scalar_fields/<observable>/<field file name>: V doubles, x fastest (GLAC/io/fieldio.cpp:137-193)
+void writeScalarField(const Parameters &P, const std::string &observable, const std::vector<double> &field,
+                      unsigned configNumber);
 void makeDirs(const std::string &path);
 
 }  // namespace glac_host

@@ -115,6 +115,17 @@ glac_status glac_flow(glac_ctx *ctx, int n_steps, double *obs);
 /* Observables of the current field (replaces MasterSamplerTopcXYZ::calculate,
  * GLAC/observables/mastersamplertopcxyz.cpp:236-384). */
 glac_status glac_measure(glac_ctx *ctx, double *obs);
+/* As glac_measure, plus the per-site densities of LatticeActionChargeDensity
+ * (GLAC/observables/latticeactionchargedensity.cpp:169-306), V doubles each in
+ * the host site order: q_density[n] = -(1/(16^2 pi^2)) sum_nu ReTr(C_0nu C_rhosigma)
+ * (sums to topc) and e_density[n] = sum ReTr(C C) (unnormalised; energy =
+ * sum / V).  obs may be NULL.  Host pointers; synchronous. */
+glac_status glac_measure_density(glac_ctx *ctx, double *obs, double *q_density, double *e_density);
+/* The Philox sweep counter of this context (advanced by every Metropolis sweep):
+ * saved beside a stored configuration, it lets a loaded chain continue its
+ * random stream where it stopped.  No counterpart in the reference. */
+glac_status glac_get_sweep(glac_ctx *ctx, uint32_t *sweep);
+glac_status glac_set_sweep(glac_ctx *ctx, uint32_t sweep);
 /* One load-and-flow pass from host memory: set the field from host_links, then
  * glac_flow(n_steps, obs) (System::flowConfigurations, GLAC/system.cpp:570-602). */
 glac_status glac_flow_configuration(glac_ctx *ctx, const double *host_links, int n_steps, double *obs);

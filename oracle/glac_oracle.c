@@ -399,6 +399,32 @@ void oracle_observables(const int N[4], const double *links, double *out) {
     out[2] = energy / (double)V;
 }
 
+/* Per-site densities of LatticeActionChargeDensity::calculate
+ * (GLAC/observables/latticeactionchargedensity.cpp:169-306): q[s] = topological
+ * charge density with the factor 1/(16^2 pi^2) (:288-291), e[s] = sum of
+ * ReTr(C C) over the six planes, unnormalised (:297-305). */
+void oracle_density(const int N[4], const double *links, double *q, double *e) {
+    long V = (long)N[0] * N[1] * N[2] * N[3];
+    double qfac = 1.0 / (16 * 16 * M_PI * M_PI);
+    for (long s = 0; s < V; s++) {
+        int c[4];
+        coords_of(N, s, c);
+        double qs = 0.0, es = 0.0;
+        for (int nu = 1; nu < 4; nu++) {
+            int rho = nu % 3 + 1, sigma = rho % 3 + 1;
+            double C1[18], C2[18], P[18];
+            clover(N, V, links, c, 0, nu, C1, P);
+            clover(N, V, links, c, rho, sigma, C2, P);
+            antiherm_traceless(C1);
+            antiherm_traceless(C2);
+            qs -= retr_mul(C1, C2);
+            es += retr_mul(C1, C1) + retr_mul(C2, C2);
+        }
+        q[s] = qs * qfac;
+        e[s] = es;
+    }
+}
+
 /* Plaquette (GLAC/observables/plaquette.cpp:26-40), factor 1/(18V) (:23). */
 double oracle_plaquette(const int N[4], const double *links) {
     long V = (long)N[0] * N[1] * N[2] * N[3];

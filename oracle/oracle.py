@@ -77,6 +77,7 @@ class Oracle:
         lib.oracle_metropolis_sweep.restype = C.c_uint64
         lib.oracle_haar_field.argtypes = [C.c_int * 4, _dp, C.c_uint64, C.c_uint32]
         lib.oracle_reunitarize.argtypes = [_dp, C.c_long]
+        lib.oracle_density.argtypes = [C.c_int * 4, _dp, _dp, _dp]
         lib.oracle_esj_link.argtypes = [_dp, _dp, C.c_double, C.c_int, C.c_int, _dp, C.c_int, C.c_uint64,
                                         C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, _dp]
         self.lib = lib
@@ -158,6 +159,13 @@ class Oracle:
         acc = self.lib.oracle_metropolis_sweep(n, out, beta, eps, nhits, seed, stream, sweep, int(bool(flips)))
         return out, int(acc)
 
+    def density(self, N, links):
+        """Per-site (q, e) densities of LatticeActionChargeDensity, V doubles each."""
+        n, V = _dims(N)
+        q, e = np.zeros(V), np.zeros(V)
+        self.lib.oracle_density(n, np.ascontiguousarray(links, np.float64), q, e)
+        return q, e
+
     def esj_link(self, U, A, beta, nhits, eps_grid, trials, seed, link_id, snapshot, stream, flips=True):
         """Expected squared jump of one link for each spread on the grid."""
         g = np.ascontiguousarray(eps_grid, np.float64)
@@ -213,6 +221,7 @@ class Reference:
         lib.ref_time_flow.restype = C.c_double
         lib.ref_time_flow_measure.argtypes = [_dp, C.c_int]
         lib.ref_time_flow_measure.restype = C.c_double
+        lib.ref_density.argtypes = [_dp, _dp, _dp, _dp]
         lib.ref_metropolis_chain.argtypes = [_dp, C.c_int, _dp]
         lib.ref_metropolis_chain.restype = C.c_double
         lib.ref_time_metropolis.argtypes = [_dp, C.c_int, C.POINTER(C.c_double)]
@@ -287,6 +296,12 @@ class Reference:
         out = np.array(links, np.float64, copy=True, order="C")
         acc = self.lib.ref_metropolis(out, int(nsweeps))
         return out, acc
+
+    def density(self, links):
+        """(q, e, [plaq, topc, energy]) of the reference's LatticeActionChargeDensity."""
+        q, e, o = np.zeros(self.V), np.zeros(self.V), np.zeros(3)
+        self.lib.ref_density(np.ascontiguousarray(links, np.float64), q, e, o)
+        return q, e, o
 
     def metropolis_chain(self, links, nsweeps):
         """nsweeps sweeps of one System: (links after, plaquette per sweep, acceptance)."""

@@ -231,6 +231,27 @@ void ref_observables_nt(const double *links, double *out) {
     for (size_t i = 0; i < 3; i++) out[i] = v[i];
 }
 
+/* LatticeActionChargeDensity::calculate (GLAC/observables/latticeactionchargedensity.cpp:169-306)
+ * as a flow sampler at a measurement index the sampling frequency skips, so
+ * nothing is written; the per-site fields are read from the sampler. */
+void ref_density(const double *links, double *q, double *e, double *obs3) {
+    std::unique_ptr<Lattice<SU3>[]> L(new Lattice<SU3>[4]);
+    to_lattice(links, L.get());
+    const int sf = Parameters::getSamplingFrequency();
+    Parameters::setSamplingFrequency(1 << 30);
+    {
+        LatticeActionChargeDensity S(true);
+        S.calculate(L.get(), 1);
+        for (unsigned long s = 0; s < g_V; s++) {
+            q[s] = S.m_topCharge.m_sites[s];
+            e[s] = S.m_energy.m_sites[s];
+        }
+        std::vector<double> v = S.getObservablesVector(1);
+        for (int i = 0; i < 3; i++) obs3[i] = v[i];
+    }
+    Parameters::setSamplingFrequency(sf);
+}
+
 /* Plaquette::calculate (GLAC/observables/plaquette.cpp:26-40). */
 double ref_plaquette(const double *links) {
     std::unique_ptr<Lattice<SU3>[]> L(new Lattice<SU3>[4]);

@@ -278,3 +278,35 @@ def test_uneven_extents_and_obs_plan(g, oracle):
         L.set_links(links)
         assert rel_err(L.measure(), oracle.observables(N, links)) < 1e-12
         assert rel_err(L.staples(), oracle.staples(N, links)) < 1e-12
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+def test_charge_density_matches_reference(g, oracle, reference, prec, tol):
+    # LatticeActionChargeDensity's per-site fields (the energyTopcFieldDensity sampler)
+    N = (4, 4, 4, 8)
+    reference.configure(4, 8, flow_eps=0.02, nflows=4)
+    links = oracle.flow(N, oracle.haar_field(N, 17), 0.02, 3)
+    q_ref, e_ref, obs_ref = reference.density(links)
+    with lattice(g, N, prec) as L:
+        L.set_links(links)
+        obs, q, e = L.measure_density()
+        assert rel_err(obs, L.measure()) < 1e-14
+    assert np.max(np.abs(q - q_ref)) < tol * np.max(np.abs(q_ref))
+    assert np.max(np.abs(e - e_ref)) < tol * np.max(np.abs(e_ref))
+    assert abs(q.sum() - obs[1]) < 1e-10 and abs(e.sum() / L.V - obs[2]) < 1e-9 * abs(obs[2])
+    assert rel_err(obs[:3], obs_ref) < tol
+
+
+def test_sweep_counter_continues_the_stream(g, oracle):
+    N = (4, 4, 4, 8)
+    start = oracle.haar_field(N, 3)
+    with lattice(g, N, "fp64", seed=11) as A, lattice(g, N, "fp64", seed=11) as B:
+        A.set_links(start)
+        A.metropolis(3)
+        mid = A.get_links()
+        A.metropolis(2)
+        B.set_links(mid)
+        B.sweep = 3  # as restored from a checkpoint sidecar
+        B.metropolis(2)
+        assert A.sweep == B.sweep == 5
+        assert np.array_equal(A.get_links(), B.get_links())

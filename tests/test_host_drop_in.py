@@ -113,3 +113,59 @@ def test_load_and_flow_matches_reference(tmp_path, oracle, reference):
     got = [read_flow(out / n / ("t2_%s_flow_config00000.dat" % n))[3, 1] for n in ("plaq", "topc", "energy")]
     assert rel_err(got, want[:3]) < 1e-12
     assert not (out / "topct").exists()
+
+
+@pytest.mark.gpu
+def test_energy_topc_field_density_run(tmp_path, oracle, reference):
+    # flowObservables ["energyTopcFieldDensity"] alone: LatticeActionChargeDensity
+    # with per-site q and E fields every samplingFrequency flow steps, one config
+    N, V = (4, 4, 4, 8), 512
+    links = oracle.haar_field(N, 78)
+    import glac_b200 as g
+    os.makedirs(tmp_path / "input")
+    g.write_field(str(tmp_path / "input" / "cfgB.bin"), N, links)
+    path, cfg = make_config(tmp_path, load_field_configs=True, field_configs=["cfgB.bin"], NFlows=4,
+                            batchName="t3", flowObservables=["energyTopcFieldDensity"], samplingFrequency=2)
+    r = subprocess.run([GLAC, path], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    sf = tmp_path / "output" / "t3" / "scalar_fields"
+    reference.configure(4, 8, flow_eps=0.01, nflows=4)
+    for step in (0, 2, 4):
+        name = "t3_b6.000000_N4_NT8_np1_config%05d.bin" % step
+        q = np.fromfile(sf / "topc" / name, dtype=np.float64)
+        e = np.fromfile(sf / "energy" / name, dtype=np.float64)
+        assert q.size == V and e.size == V
+        qr, er, _ = reference.density(reference.flow(links, step) if step else links)
+        assert np.max(np.abs(q - qr)) < 1e-12 * np.max(np.abs(qr))
+        assert np.max(np.abs(e - er)) < 1e-12 * np.max(np.abs(er))
+    for step in (1, 3):
+        assert not (sf / "topc" / ("t3_b6.000000_N4_NT8_np1_config%05d.bin" % step)).exists()
+    fo = tmp_path / "output" / "t3" / "flow_observables"
+    topc = read_flow(fo / "topc" / "t3_topc_flow_config00000.dat")
+    q4 = np.fromfile(sf / "topc" / "t3_b6.000000_N4_NT8_np1_config00004.bin", dtype=np.float64)
+    assert abs(topc[4, 1] - q4.sum()) < 1e-12
+    assert not (fo / "topct").exists()
+
+
+@pytest.mark.gpu
+def test_stored_configuration_carries_its_random_stream(tmp_path):
+    # a chain stopped after config 0 and resumed from its file continues with the
+    # same random numbers as the uninterrupted chain
+    path, cfg = make_config(tmp_path, NCf=2, NCor=3, NTherm=4, NFlows=0, batchName="t4")
+    r = subprocess.run([GLAC, path], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    fc = tmp_path / "output" / "t4" / "field_configurations"
+    side = open(fc / "t4_b6.000000_N4_NT8_np1_config00000.bin.rng").read().split()
+    assert side[0] == "metropolisSeed" and float(side[1]) == 12 and side[2] == "sweep" and int(side[3]) == 4 + 3
+    os.makedirs(tmp_path / "input")
+    import shutil
+    for ext in ("", ".rng"):
+        shutil.copy(fc / ("t4_b6.000000_N4_NT8_np1_config00000.bin" + ext), tmp_path / "input" / ("c0.bin" + ext))
+    path2, _ = make_config(tmp_path, NCf=1, NCor=3, NTherm=0, NFlows=0, batchName="t5", load_config_and_run="c0.bin")
+    r = subprocess.run([GLAC, path2], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    import glac_b200 as g
+    N = (4, 4, 4, 8)
+    a = g.read_field(str(fc / "t4_b6.000000_N4_NT8_np1_config00001.bin"), N)
+    b = g.read_field(str(tmp_path / "output" / "t5" / "field_configurations" / "t5_b6.000000_N4_NT8_np1_config00000.bin"), N)
+    assert np.array_equal(a, b)
