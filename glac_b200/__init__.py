@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
     # learned proposal spread
     L.glac_copy_field.argtypes = [P, P]
     L.glac_measure_density.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.glac_measure_weinberg.argtypes = [P, C.c_void_p]
     L.glac_get_sweep.argtypes = [P, C.POINTER(C.c_uint32)]
     L.glac_set_sweep.argtypes = [P, C.c_uint32]
     L.glac_set_proposal_net.argtypes = [P, C.c_void_p, C.c_double, C.c_double]
@@ -334,6 +335,12 @@ class Lattice:
         q, e = np.empty(self.V), np.empty(self.V)
         self._ck(lib().glac_measure_density(self._ctx, obs.ctypes.data, q.ctypes.data, e.ctypes.data))
         return obs, q, e
+
+    def measure_weinberg(self):
+        """SuperSampler observables: [plaq, topc, energy, weinberg, topct[Nt], weinbergt[Nt]]."""
+        out = np.empty(4 + 2 * self.Nt)
+        self._ck(lib().glac_measure_weinberg(self._ctx, out.ctypes.data))
+        return out
 
     @property
     def sweep(self) -> int:

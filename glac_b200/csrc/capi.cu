@@ -23,6 +23,7 @@ struct glac_ctx {
     int cur = 0;
     void *force = nullptr;
     double *partial = nullptr;
+    double *partial4 = nullptr;  // SuperSampler partials, 4 per block (allocated on first use)
     double *obs_dev = nullptr;
     size_t obs_cap = 0;  // doubles in obs_dev
     unsigned long long *acc_dev = nullptr;
@@ -224,6 +225,7 @@ void glac_destroy(glac_ctx *c) {
     for (int i = 0; i < 2; i++) if (c->field[i]) cudaFree(c->field[i]);
     if (c->force) cudaFree(c->force);
     if (c->partial) cudaFree(c->partial);
+    if (c->partial4) cudaFree(c->partial4);
     if (c->obs_dev) cudaFree(c->obs_dev);
     if (c->acc_dev) cudaFree(c->acc_dev);
     if (c->staging) cudaFree(c->staging);
@@ -452,6 +454,27 @@ glac_status glac_measure_density(glac_ctx *c, double *obs, double *q_density, do
         if (obs) ck(cudaMemcpyAsync(obs, c->obs_dev, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H");
         ck(cudaMemcpyAsync(q_density, dq, V * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H q");
         ck(cudaMemcpyAsync(e_density, de, V * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H e");
+        ck(cudaStreamSynchronize(c->stream), "sync");
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_measure_weinberg(glac_ctx *c, double *obs) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        if (!obs) {
+            c->err = "null output";
+            return GLAC_ERR_ARG;
+        }
+        const size_t n = 4 + 2 * (size_t)c->g.N[3];
+        ensure_obs(c, n);
+        if (!c->partial4) ck(cudaMalloc(&c->partial4, 4 * (size_t)c->plan.nblocks * sizeof(double)), "partials");
+        if (c->d.precision == GLAC_FP64) launch_weinberg(c->g, f64(c, c->cur), c->plan, c->partial4, c->obs_dev, c->stream);
+        else launch_weinberg(c->g, f32(c, c->cur), c->plan, c->partial4, c->obs_dev, c->stream);
+        ck_launch("weinberg");
+        c->launches += 2;
+        ck(cudaMemcpyAsync(obs, c->obs_dev, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H");
         ck(cudaStreamSynchronize(c->stream), "sync");
         return GLAC_OK;
     });

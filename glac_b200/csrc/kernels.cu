@@ -646,6 +646,119 @@ template void launch_observables<float>(const Geom &, const LinkField<float> &, 
                                         double *, int, cudaStream_t);
 
 // ---------------------------------------------------------------------------
+// SuperSampler (GLAC/observables/supersampler.cpp:298-496): the observables
+// above plus the Weinberg operator.  With the six projected clovers G of a
+// site, for nu = 1..3 and (rho, sigma) the cyclic complement of nu:
+//   w(t) -= ReTr[(sum_{lambda != nu} G_{0 lambda} G_{nu lambda}) G_{rho sigma}],
+// factor 2 * 8 * 8 / (3 * 16^3) (:13).  G_{b a} = G_{a b}^+ for the
+// orientations the reference does not store (:421-433).  Partials: 4 per block.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_observables_weinberg(Geom g, LinkField<T> L, int nb, int Bv,
+                                                              double *partial) {
+    const int b = blockIdx.x;
+    const int t = b / (2 * nb);
+    const int p = (b / nb) & 1;
+    const int j = b % nb;
+    const int half_slice = g.Vh / g.N[3];
+    const bool valid = (int)threadIdx.x < Bv;
+    const int s = t * half_slice + j * Bv + (valid ? (int)threadIdx.x : 0);
+    double plaq = 0.0, en = 0.0, qt = 0.0, wt = 0.0;
+    if (valid) {
+        const Site n = site_from_ps(g, p, s);
+        AH8<T> G0[4], Gc[4];  // G0[nu] = G_{0 nu}; Gc[nu] = G_{rho sigma} of nu's complement
+#pragma unroll 1
+        for (int nu = 1; nu < 4; nu++) {
+            const int rho = nu % 3 + 1, sigma = rho % 3 + 1;
+            T pl1, pl2;
+            G0[nu] = clover_ah(L, g, n, p, 0, nu, pl1);
+            Gc[nu] = clover_ah(L, g, n, p, rho, sigma, pl2);
+            plaq += (double)pl1 + (double)pl2;
+            qt -= (double)retr_ah(G0[nu], Gc[nu]);
+            en += (double)retr_ah(G0[nu], G0[nu]) + (double)retr_ah(Gc[nu], Gc[nu]);
+        }
+        // G_{a b} for spatial a != b from the stored G_{23} = Gc[1], G_{31} = Gc[2], G_{12} = Gc[3]
+        auto spatial = [&](int a, int c) -> M3<T> {
+            // (a, c) in {(1,2),(2,3),(3,1)} is stored as Gc[the third index]; the reverse is its dagger
+            const int k = 6 - a - c;
+            const bool stored = (c == a % 3 + 1);
+            const M3<T> m = ah_to_m3(Gc[k]);
+            return stored ? m : dagger(m);
+        };
+#pragma unroll 1
+        for (int nu = 1; nu < 4; nu++) {
+            M3<T> acc;
+            set_zero(acc);
+#pragma unroll 1
+            for (int lam = 1; lam < 4; lam++) {
+                if (lam == nu) continue;
+                acc_mul(acc, ah_to_m3(G0[lam]), spatial(nu, lam));
+            }
+            wt -= (double)retr_mul(acc, ah_to_m3(Gc[nu]));
+        }
+    }
+    __shared__ double sh[4][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    plaq = warp_sum_d(plaq);
+    en = warp_sum_d(en);
+    qt = warp_sum_d(qt);
+    wt = warp_sum_d(wt);
+    if (lane == 0) { sh[0][wid] = plaq; sh[1][wid] = en; sh[2][wid] = qt; sh[3][wid] = wt; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double a = 0.0, e = 0.0, q = 0.0, w = 0.0;
+        for (int k = 0; k < nw; k++) { a += sh[0][k]; e += sh[1][k]; q += sh[2][k]; w += sh[3][k]; }
+        partial[4 * b] = a;
+        partial[4 * b + 1] = e;
+        partial[4 * b + 2] = q;
+        partial[4 * b + 3] = w;
+    }
+}
+
+// out = [plaq, topc, energy, weinberg, topct[Nt], weinbergt[Nt]]
+__global__ void k_weinberg_finalize(int Nt, int nb, int V, const double *partial, double *out) {
+    __shared__ double sp[1024], se[1024], sq[1024], sw[1024];
+    for (int t = threadIdx.x; t < Nt; t += blockDim.x) {
+        double a = 0.0, e = 0.0, q = 0.0, w = 0.0;
+        for (int k = 0; k < 2 * nb; k++) {
+            const double *pp = partial + 4 * ((size_t)t * 2 * nb + k);
+            a += pp[0];
+            e += pp[1];
+            q += pp[2];
+            w += pp[3];
+        }
+        sp[t] = a; se[t] = e; sq[t] = q; sw[t] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double qfac = 1.0 / (16 * 16 * M_PI * M_PI), wfac = 2 * 8.0 * 8.0 / (3 * 16 * 16 * 16);
+        double a = 0.0, e = 0.0, q = 0.0, w = 0.0;
+        for (int t = 0; t < Nt; t++) { a += sp[t]; e += se[t]; q += sq[t]; w += sw[t]; }
+        out[0] = a / (18.0 * (double)V);
+        out[1] = q * qfac;
+        out[2] = e / (double)V;
+        out[3] = w * wfac;
+        for (int t = 0; t < Nt; t++) {
+            out[4 + t] = sq[t] * qfac;
+            out[4 + Nt + t] = sw[t] * wfac;
+        }
+    }
+}
+
+template <typename T>
+void launch_weinberg(const Geom &g, const LinkField<T> &L, const ObsPlan &plan, double *partial4, double *out,
+                     cudaStream_t st) {
+    if (g.N[3] > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
+    k_observables_weinberg<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial4);
+    k_weinberg_finalize<<<1, 256, 0, st>>>(g.N[3], plan.nb, g.V, partial4, out);
+}
+template void launch_weinberg<double>(const Geom &, const LinkField<double> &, const ObsPlan &, double *, double *,
+                                      cudaStream_t);
+template void launch_weinberg<float>(const Geom &, const LinkField<float> &, const ObsPlan &, double *, double *,
+                                     cudaStream_t);
+
+// ---------------------------------------------------------------------------
 // Start fields, reunitarisation, layout conversion
 // ---------------------------------------------------------------------------
 template <typename T> __device__ __forceinline__ M3<T> to_t(const M3<double> &a) {

@@ -74,6 +74,10 @@ template <typename T>
 void launch_esj(const Geom &g, const LinkField<T> &L, double beta, int nhits, int n_eps, const float *eps_grid_dev,
                 int trials, int stride, int offset, int ns, uint64_t seed, uint32_t snapshot, uint32_t stream_id,
                 bool flips, float *feat, float *esj, uint32_t *ids, cudaStream_t st);
+// SuperSampler observables: [plaq, topc, energy, weinberg, topct[Nt], weinbergt[Nt]]; partial4: 4 per block.
+template <typename T>
+void launch_weinberg(const Geom &g, const LinkField<T> &L, const ObsPlan &plan, double *partial4, double *out,
+                     cudaStream_t st);
 // Observables plus per-site topological-charge and energy densities (V doubles each, lexicographic).
 template <typename T>
 void launch_observables_density(const Geom &g, const LinkField<T> &L, const ObsPlan &plan, double *partial,

@@ -3,6 +3,7 @@
 
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -133,15 +134,17 @@ void ObservableStorer::run_statistics() {
 
 // GLAC/system.cpp:62-125
 Sampler select_sampler(const std::vector<std::string> &names) {
-    bool plaq = false, topc = false, energy = false, topct = false, density = false;
+    bool plaq = false, topc = false, energy = false, topct = false, density = false, weinberg = false;
     for (const std::string &n : names) {
         if (n == "plaq") plaq = true;
         else if (n == "topc") topc = true;
         else if (n == "energy") energy = true;
         else if (n == "topct") topct = true;
         else if (n == "energyTopcFieldDensity") density = true;
+        else if (n == "weinberg") weinberg = true;
         else throw std::runtime_error("observable \"" + n + "\" is not provided by this implementation");
     }
+    if (weinberg) return Sampler::Super;
     if ((topc || energy) && !topct) return Sampler::Master;
     if (plaq && !topc && !energy && !topct) return Sampler::Plaquette;
     if (density && !plaq && !topc && !energy && !topct) return Sampler::ChargeDensity;
@@ -150,8 +153,22 @@ Sampler select_sampler(const std::vector<std::string> &names) {
 std::vector<std::string> sampler_names(Sampler s, bool flow) {
     if (s == Sampler::Plaquette) return {"plaq"};
     if (s == Sampler::ChargeDensity) return {"plaq", "topc", "energy"};
+    if (s == Sampler::Super)  // GLAC/observables/supersampler.cpp:134-174
+        return flow ? std::vector<std::string>{"plaq", "topc", "weinberg", "energy", "topct", "weinbergt"}
+                    : std::vector<std::string>{"plaq", "topc", "energy", "weinberg"};
     if (s == Sampler::Master || !flow) return {"plaq", "topc", "energy"};
     return {"plaq", "topc", "energy", "topct"};
+}
+
+size_t row_width(Sampler s, unsigned Nt) { return s == Sampler::Super ? 4 + 2 * (size_t)Nt : 3 + (size_t)Nt; }
+size_t row_offset(Sampler s, const std::string &name, unsigned Nt) {
+    if (name == "plaq") return 0;
+    if (name == "topc") return 1;
+    if (name == "energy") return 2;
+    if (name == "weinberg") return 3;
+    if (name == "topct") return s == Sampler::Super ? 4 : 3;
+    if (name == "weinbergt") return 4 + (size_t)Nt;
+    throw std::runtime_error("no observable " + name);
 }
 
 void makeDirs(const std::string &path) {
@@ -250,7 +267,12 @@ System::System(const Parameters &p) : P(p) {
 }
 
 void System::measureInto(glac_ctx *c, Sampler s, unsigned index, bool write, std::vector<double> &obs) {
-    obs.resize(3 + P.NTemporal);
+    obs.resize(row_width(s, P.NTemporal));
+    if (s == Sampler::Super) {
+        if (glac_measure_weinberg(c, obs.data()) != GLAC_OK)
+            throw std::runtime_error(std::string("measure: ") + glac_last_error(c));
+        return;
+    }
     if (s != Sampler::ChargeDensity || !write) {
         if (glac_measure(c, obs.data()) != GLAC_OK) throw std::runtime_error(std::string("measure: ") + glac_last_error(c));
         return;
@@ -322,14 +344,14 @@ void System::storeConfigObservables(unsigned index, const std::vector<double> &o
         for (const std::string &n : names) cfgObs.push_back(ObservableStorer{n, {}});
     for (size_t k = 0; k < names.size(); k++) {
         if (cfgObs[k].values.size() <= index) cfgObs[k].values.resize(index + 1, 0.0);
-        cfgObs[k].values[index] = obs[k];
+        cfgObs[k].values[index] = obs[row_offset(cfgSampler, names[k], P.NTemporal)];
     }
 }
 
 // GLAC/system.cpp:262-319
 void System::thermalize() {
     std::printf("\nInitiating thermalization.");
-    std::vector<double> obs(3 + P.NTemporal);
+    std::vector<double> obs(row_width(cfgSampler, P.NTemporal));
     if (P.storeThermalizationObservables) {
         NThermSteps = 1 + P.NTherm;
         measureInto(ctx, cfgSampler, 0, true, obs);
@@ -359,7 +381,7 @@ void System::runMetropolis() {
     std::printf("\ni    %-20s Avg.Update-time  Accept/reject", "observables");
     acceptanceScore = 0.0;
     double seconds = 0.0;
-    std::vector<double> obs(3 + P.NTemporal);
+    std::vector<double> obs(row_width(cfgSampler, P.NTemporal));
     for (unsigned iConfig = 0; iConfig < P.NCf; iConfig++) {
         const auto t0 = std::chrono::steady_clock::now();
         double a = 0;
@@ -369,7 +391,13 @@ void System::runMetropolis() {
         checkLattice("in system right before copying to flow lattice");
         if (P.NFlows != 0) {
             flowConfiguration(iConfig);  // flows a copy; the chain field stays in ctx
-            obs = lastFlowT0;
+            // the flow sampler's t = 0 values, by name, into the config sampler's row
+            obs.assign(row_width(cfgSampler, P.NTemporal), 0.0);
+            const std::vector<std::string> fnames = sampler_names(flowSampler, true);
+            for (const std::string &n : sampler_names(cfgSampler, false))
+                if (std::find(fnames.begin(), fnames.end(), n) != fnames.end() || n == "plaq" || n == "topc" ||
+                    n == "energy")
+                    obs[row_offset(cfgSampler, n, P.NTemporal)] = lastFlowT0[row_offset(flowSampler, n, P.NTemporal)];
         } else {
             measureInto(ctx, cfgSampler, iConfig + NThermSteps, true, obs);
         }
@@ -410,9 +438,9 @@ void System::flowConfiguration(unsigned iConfig) {
         ck(glac_create(&d, &flowCtx), "glac_create (flow lattice)");
     }
     ck(glac_copy_field(flowCtx, ctx), "copy to flow lattice");
-    const unsigned per = 3 + P.NTemporal;
+    const size_t per = row_width(flowSampler, P.NTemporal);
     std::vector<double> obs((size_t)(P.NFlows + 1) * per);
-    if (flowSampler == Sampler::ChargeDensity) {
+    if (flowSampler == Sampler::ChargeDensity || flowSampler == Sampler::Super) {
         // step by step: the per-site fields every samplingFrequency flow steps
         // (LatticeActionChargeDensity::calculate, :277-294; file number = flow step)
         std::vector<double> o;
@@ -433,13 +461,13 @@ void System::flowConfiguration(unsigned iConfig) {
             std::printf("\n%-4u %-3.3f  %-20.15f %-20.15f %-20.15f", i, i * P.flowEpsilon, obs[(size_t)i * per],
                         obs[(size_t)i * per + 1], obs[(size_t)i * per + 2]);
     for (const std::string &name : sampler_names(flowSampler, true)) {
-        if (name == "topct") {
+        const size_t k = row_offset(flowSampler, name, P.NTemporal);
+        if (name == "topct" || name == "weinbergt") {
             std::vector<double> m((size_t)(P.NFlows + 1) * P.NTemporal);
             for (unsigned i = 0; i < P.NFlows + 1; i++)
-                for (unsigned t = 0; t < P.NTemporal; t++) m[(size_t)i * P.NTemporal + t] = obs[(size_t)i * per + 3 + t];
+                for (unsigned t = 0; t < P.NTemporal; t++) m[(size_t)i * P.NTemporal + t] = obs[(size_t)i * per + k + t];
             writeMatrixToFile(P, name, m, iConfig, P.NTemporal);
         } else {
-            const int k = name == "plaq" ? 0 : name == "topc" ? 1 : 2;
             std::vector<double> v(P.NFlows + 1);
             for (unsigned i = 0; i < P.NFlows + 1; i++) v[i] = obs[(size_t)i * per + k];
             writeFlowObservableToFile(P, name, v, iConfig);

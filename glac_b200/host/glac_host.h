@@ -65,9 +65,14 @@ struct ObservableStorer {
 // three-observable MasterSampler, MasterSamplerTopcXYZ (adds topct), or
 // LatticeActionChargeDensity (energyTopcFieldDensity alone: per-site q and E
 // fields written to scalar_fields/).
-enum class Sampler { Plaquette, Master, MasterTopcXYZ, ChargeDensity };
+// "weinberg" anywhere in the list selects SuperSampler (adds weinberg, weinbergt).
+enum class Sampler { Plaquette, Master, MasterTopcXYZ, ChargeDensity, Super };
 Sampler select_sampler(const std::vector<std::string> &names);
 std::vector<std::string> sampler_names(Sampler s, bool flow);
+// Layout of a measurement row: scalars [plaq, topc, energy(, weinberg)], then
+// topct[Nt] (and weinbergt[Nt] for SuperSampler).
+size_t row_width(Sampler s, unsigned Nt);
+size_t row_offset(Sampler s, const std::string &name, unsigned Nt);
 
 class System {
 public:

@@ -121,6 +121,10 @@ glac_status glac_measure(glac_ctx *ctx, double *obs);
  * (sums to topc) and e_density[n] = sum ReTr(C C) (unnormalised; energy =
  * sum / V).  obs may be NULL.  Host pointers; synchronous. */
 glac_status glac_measure_density(glac_ctx *ctx, double *obs, double *q_density, double *e_density);
+/* SuperSampler::calculate (GLAC/observables/supersampler.cpp:298-496), the
+ * sampler the observable list "weinberg" selects: obs = [plaq, topc, energy,
+ * weinberg, topct[Nt], weinbergt[Nt]] (4 + 2 Nt doubles, host). */
+glac_status glac_measure_weinberg(glac_ctx *ctx, double *obs);
 /* The Philox sweep counter of this context (advanced by every Metropolis sweep):
  * saved beside a stored configuration, it lets a loaded chain continue its
  * random stream where it stopped.  No counterpart in the reference. */

@@ -399,6 +399,59 @@ void oracle_observables(const int N[4], const double *links, double *out) {
     out[2] = energy / (double)V;
 }
 
+/* SuperSampler::calculate (GLAC/observables/supersampler.cpp:298-496):
+ * out = [plaq, topc, energy, weinberg, topct[Nt], weinbergt[Nt]].  The six
+ * projected clovers per site; for nu = 1..3, temp = sum over spatial lambda != nu
+ * of G_{0 lambda} G_{nu lambda} (G_{b a} = G_{a b}^+ where only (a, b) is
+ * formed, :421-433), w(t) -= ReTr(temp G_{rho sigma}); factor 2*8*8/(3*16^3) (:13). */
+void oracle_weinberg(const int N[4], const double *links, double *out) {
+    long V = (long)N[0] * N[1] * N[2] * N[3];
+    int Nt = N[3];
+    double plaq = 0.0, energy = 0.0;
+    double *qt = out + 4, *wt = out + 4 + Nt;
+    for (int t = 0; t < Nt; t++) qt[t] = wt[t] = 0.0;
+    for (long s = 0; s < V; s++) {
+        int c[4];
+        coords_of(N, s, c);
+        double G[4][4][18]; /* G[a][b], all ordered spatial/temporal pairs that are used */
+        for (int nu = 1; nu < 4; nu++) {
+            int rho = nu % 3 + 1, sigma = rho % 3 + 1;
+            double P[18];
+            clover(N, V, links, c, 0, nu, G[0][nu], P);
+            plaq += retr(P);
+            clover(N, V, links, c, rho, sigma, G[rho][sigma], P);
+            plaq += retr(P);
+            antiherm_traceless(G[0][nu]);
+            antiherm_traceless(G[rho][sigma]);
+            dag(G[rho][sigma], G[sigma][rho]);
+            qt[c[3]] -= retr_mul(G[0][nu], G[rho][sigma]);
+            energy += retr_mul(G[0][nu], G[0][nu]) + retr_mul(G[rho][sigma], G[rho][sigma]);
+        }
+        for (int nu = 1; nu < 4; nu++) {
+            int rho = nu % 3 + 1, sigma = rho % 3 + 1;
+            double T[18] = {0}, M[18];
+            for (int lam = 1; lam < 4; lam++) {
+                if (lam == nu) continue;
+                mm(G[0][lam], G[nu][lam], M);
+                madd(T, M);
+            }
+            wt[c[3]] -= retr_mul(T, G[rho][sigma]);
+        }
+    }
+    double qfac = 1.0 / (16 * 16 * M_PI * M_PI), wfac = 2 * 8.0 * 8.0 / (3 * 16 * 16 * 16);
+    double topc = 0.0, w = 0.0;
+    for (int t = 0; t < Nt; t++) {
+        topc += qt[t];
+        w += wt[t];
+        qt[t] *= qfac;
+        wt[t] *= wfac;
+    }
+    out[0] = plaq / (18.0 * (double)V);
+    out[1] = topc * qfac;
+    out[2] = energy / (double)V;
+    out[3] = w * wfac;
+}
+
 /* Per-site densities of LatticeActionChargeDensity::calculate
  * (GLAC/observables/latticeactionchargedensity.cpp:169-306): q[s] = topological
  * charge density with the factor 1/(16^2 pi^2) (:288-291), e[s] = sum of

@@ -52,6 +52,9 @@ void oracle_flow(const int N[4], double *links, double eps, int nsteps, int expk
 /* out = [plaq, topc, energy, topct[0..Nt-1]]
  * (GLAC/observables/mastersamplertopcxyz.cpp:236-384). */
 void oracle_observables(const int N[4], const double *links, double *out);
+/* SuperSampler observables [plaq, topc, energy, weinberg, topct[Nt], weinbergt[Nt]]
+ * (GLAC/observables/supersampler.cpp:298-496). */
+void oracle_weinberg(const int N[4], const double *links, double *out);
 /* Per-site topological charge density q (with 1/(16^2 pi^2)) and unnormalised
  * energy density e, V doubles each (GLAC/observables/latticeactionchargedensity.cpp:169-306). */
 void oracle_density(const int N[4], const double *links, double *q, double *e);

@@ -78,6 +78,7 @@ class Oracle:
         lib.oracle_haar_field.argtypes = [C.c_int * 4, _dp, C.c_uint64, C.c_uint32]
         lib.oracle_reunitarize.argtypes = [_dp, C.c_long]
         lib.oracle_density.argtypes = [C.c_int * 4, _dp, _dp, _dp]
+        lib.oracle_weinberg.argtypes = [C.c_int * 4, _dp, _dp]
         lib.oracle_esj_link.argtypes = [_dp, _dp, C.c_double, C.c_int, C.c_int, _dp, C.c_int, C.c_uint64,
                                         C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, _dp]
         self.lib = lib
@@ -159,6 +160,13 @@ class Oracle:
         acc = self.lib.oracle_metropolis_sweep(n, out, beta, eps, nhits, seed, stream, sweep, int(bool(flips)))
         return out, int(acc)
 
+    def weinberg(self, N, links):
+        """SuperSampler observables [plaq, topc, energy, weinberg, topct[Nt], weinbergt[Nt]]."""
+        n, _ = _dims(N)
+        out = np.zeros(4 + 2 * int(N[3]))
+        self.lib.oracle_weinberg(n, np.ascontiguousarray(links, np.float64), out)
+        return out
+
     def density(self, N, links):
         """Per-site (q, e) densities of LatticeActionChargeDensity, V doubles each."""
         n, V = _dims(N)
@@ -222,6 +230,7 @@ class Reference:
         lib.ref_time_flow_measure.argtypes = [_dp, C.c_int]
         lib.ref_time_flow_measure.restype = C.c_double
         lib.ref_density.argtypes = [_dp, _dp, _dp, _dp]
+        lib.ref_supersampler.argtypes = [_dp, _dp]
         lib.ref_metropolis_chain.argtypes = [_dp, C.c_int, _dp]
         lib.ref_metropolis_chain.restype = C.c_double
         lib.ref_time_metropolis.argtypes = [_dp, C.c_int, C.POINTER(C.c_double)]
@@ -296,6 +305,12 @@ class Reference:
         out = np.array(links, np.float64, copy=True, order="C")
         acc = self.lib.ref_metropolis(out, int(nsweeps))
         return out, acc
+
+    def supersampler(self, links):
+        """The reference's SuperSampler: [plaq, topc, energy, weinberg, topct[Nt], weinbergt[Nt]]."""
+        out = np.zeros(4 + 2 * self.N[3])
+        self.lib.ref_supersampler(np.ascontiguousarray(links, np.float64), out)
+        return out
 
     def density(self, links):
         """(q, e, [plaq, topc, energy]) of the reference's LatticeActionChargeDensity."""

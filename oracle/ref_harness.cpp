@@ -231,6 +231,25 @@ void ref_observables_nt(const double *links, double *out) {
     for (size_t i = 0; i < 3; i++) out[i] = v[i];
 }
 
+/* SuperSampler::calculate (GLAC/observables/supersampler.cpp:298-496) at
+ * measurement 0: out = [plaq, topc, energy, weinberg, topct[Nt], weinbergt[Nt]]. */
+void ref_supersampler(const double *links, double *out) {
+    std::unique_ptr<Lattice<SU3>[]> L(new Lattice<SU3>[4]);
+    to_lattice(links, L.get());
+    SuperSampler S(true);
+    S.reset();
+    S.calculate(L.get(), 0);
+    const int Nt = g_N[3];
+    out[0] = (*S.m_plaqObservable)[0];
+    out[1] = (*S.m_topcObservable)[0];
+    out[2] = (*S.m_energyObservable)[0];
+    out[3] = (*S.m_wObservable)[0];
+    for (int t = 0; t < Nt; t++) {
+        out[4 + t] = (*S.m_topctObservable)[t];
+        out[4 + Nt + t] = (*S.m_wtObservable)[t];
+    }
+}
+
 /* LatticeActionChargeDensity::calculate (GLAC/observables/latticeactionchargedensity.cpp:169-306)
  * as a flow sampler at a measurement index the sampling frequency skips, so
  * nothing is written; the per-site fields are read from the sampler. */

@@ -310,3 +310,18 @@ def test_sweep_counter_continues_the_stream(g, oracle):
         B.metropolis(2)
         assert A.sweep == B.sweep == 5
         assert np.array_equal(A.get_links(), B.get_links())
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+def test_weinberg_matches_reference(g, oracle, reference, prec, tol):
+    N = (4, 4, 4, 8)
+    reference.configure(4, 8, flow_eps=0.02, nflows=4)
+    for seed in (19, 23):
+        links = oracle.flow(N, oracle.haar_field(N, seed), 0.02, 3)
+        want = reference.supersampler(links)
+        with lattice(g, N, prec) as L:
+            L.set_links(links)
+            got = L.measure_weinberg()
+            base = L.measure()
+        assert rel_err(got, want) < tol
+        assert rel_err(got[[0, 1, 2]], base[:3]) < 1e-13 and rel_err(got[4:12], base[3:]) < 1e-12

@@ -169,3 +169,23 @@ def test_stored_configuration_carries_its_random_stream(tmp_path):
     a = g.read_field(str(fc / "t4_b6.000000_N4_NT8_np1_config00001.bin"), N)
     b = g.read_field(str(tmp_path / "output" / "t5" / "field_configurations" / "t5_b6.000000_N4_NT8_np1_config00000.bin"), N)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_weinberg_sampler_files_match_reference(tmp_path, oracle, reference):
+    N = (4, 4, 4, 8)
+    links = oracle.haar_field(N, 79)
+    import glac_b200 as g
+    os.makedirs(tmp_path / "input")
+    g.write_field(str(tmp_path / "input" / "cfgW.bin"), N, links)
+    path, cfg = make_config(tmp_path, load_field_configs=True, field_configs=["cfgW.bin"], NFlows=3,
+                            batchName="t6", flowObservables=["plaq", "topc", "energy", "weinberg"])
+    r = subprocess.run([GLAC, path], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    reference.configure(4, 8, flow_eps=0.01, nflows=3)
+    want = reference.supersampler(reference.flow(links, 3))
+    fo = tmp_path / "output" / "t6" / "flow_observables"
+    row = {n: read_flow(fo / n / ("t6_%s_flow_config00000.dat" % n))[3, 1:] for n in
+           ("plaq", "topc", "energy", "weinberg", "topct", "weinbergt")}
+    got = np.concatenate([row["plaq"], row["topc"], row["energy"], row["weinberg"], row["topct"], row["weinbergt"]])
+    assert rel_err(got, want) < 1e-11
