@@ -75,7 +75,7 @@ GLAC_FLOW_KERNEL(k_flow_stage_r80, __maxnreg__(80))
 const int kFlowRegs[2][kMaxVariants] = {{0, 128, 0, -1}, {0, 80, 0, -1}};
 const int kFlowShape[2][kMaxVariants] = {{0, 0, 1, 0}, {0, 0, 1, 0}};
 const int kMetroRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 96, 80, 128}};
-const int kObsRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 128, -1, -1}};
+const int kObsRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 128, 168, -1}};
 
 int num_variants(Family f, bool fp32) {
     const int(*t)[kMaxVariants] = f == FAM_FLOW ? kFlowRegs : f == FAM_METRO ? kMetroRegs : kObsRegs;
@@ -453,9 +453,12 @@ ObsPlan make_obs_plan(const Geom &g) {
 
 // Clover of the (mu, nu) plane at n, projected: F = (C - C^+) - 1/3 i ImTr(C - C^+),
 // returned in the 8-real form; *plaq = ReTr(leaf1).  Links are re-read from
-// L1/L2 rather than held, to keep register pressure low.
+// L1/L2 rather than held, to keep register pressure low.  Not inlined: with
+// its own register allocation the calling kernels fit a 128-register cap
+// (4 blocks of 128 per SM) with a small spill, where the inlined form needs
+// ~180 registers (2 blocks); the autotuner picks between the two caps.
 template <typename T>
-__device__ __forceinline__ AH8<T> clover_ah(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu,
+__device__ __noinline__ AH8<T> clover_ah(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu,
                                             int nu, T &plaq) {
     const int q = p ^ 1;
     const int s_n = n.lex >> 1;
@@ -467,18 +470,19 @@ __device__ __forceinline__ AH8<T> clover_ah(const LinkField<T> &L, const Geom &g
     const int s_mm = lex_step2(g, n, mu, -1, nu, -1) >> 1;   // n-mu-nu   (p)
     const int s_mp = lex_step2(g, n, mu, -1, nu, +1) >> 1;   // n-mu+nu   (p)
     M3<T> C;
-    // compiler fences between the leaves keep their loads from being hoisted
-    // together, which would multiply the live registers
+    // Each leaf is a left-to-right chain that brings in one link per product,
+    // so one product and one link are live at a time; compiler fences between
+    // the leaves keep their loads from being hoisted together.
     {   // leaf1 = U_mu(n) U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+
-        const M3<T> P = mul(L.load(mu, p, s_n), L.load(nu, q, s_mup));
-        const M3<T> W = mul(L.load(nu, p, s_n), L.load(mu, q, s_nup));
-        C = mul_nd(P, W);
+        M3<T> t = mul(L.load(mu, p, s_n), L.load(nu, q, s_mup));
+        t = mul_nd(t, L.load(mu, q, s_nup));
+        C = mul_nd(t, L.load(nu, p, s_n));
         plaq = retr(C);
     }
     asm volatile("" ::: "memory");
     {   // leaf2 = U_mu(n) U_nu(n+mu-nu)^+ U_mu(n-nu)^+ U_nu(n-nu)
-        const M3<T> Y = mul(L.load(mu, q, s_num), L.load(nu, p, s_pm));
-        const M3<T> t = mul_nd(L.load(mu, p, s_n), Y);
+        M3<T> t = mul_nd(L.load(mu, p, s_n), L.load(nu, p, s_pm));
+        t = mul_nd(t, L.load(mu, q, s_num));
         sub_from(C, mul(t, L.load(nu, q, s_num)));
     }
     asm volatile("" ::: "memory");
@@ -546,6 +550,7 @@ __device__ __forceinline__ void observables_body(const Geom &g, const LinkField<
             const int rho = nu % 3 + 1, sigma = rho % 3 + 1;
             T pl1, pl2;
             const AH8<T> F1 = clover_ah(L, g, n, p, 0, nu, pl1);
+            asm volatile("" ::: "memory");  // one clover at a time: bounds the live registers
             const AH8<T> F2 = clover_ah(L, g, n, p, rho, sigma, pl2);
             plaq += (double)pl1 + (double)pl2;
             qt -= (double)retr_ah(F1, F2);
@@ -580,6 +585,7 @@ __device__ __forceinline__ void observables_body(const Geom &g, const LinkField<
         observables_body<T>(g, L, nb, Bv, partial, blockIdx.x);                                        \
     }
 GLAC_OBS_KERNEL(k_observables, __launch_bounds__(256))
+GLAC_OBS_KERNEL(k_observables_r168, __maxnreg__(168))
 GLAC_OBS_KERNEL(k_observables_r128, __maxnreg__(128))
 GLAC_OBS_KERNEL(k_observables_r96, __maxnreg__(96))
 #undef GLAC_OBS_KERNEL
@@ -618,6 +624,12 @@ void launch_observables(const Geom &g, const LinkField<T> &L, const ObsPlan &pla
                         int variant, cudaStream_t st) {
     if (g.N[3] > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
     switch (variant_regs(FAM_OBS, sizeof(T) == 4, variant)) {
+    case 168:
+        if constexpr (sizeof(T) == 4) {
+            k_observables_r168<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial);
+            break;
+        }
+        [[fallthrough]];
     case 128: k_observables_r128<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial); break;
     case 96: k_observables_r96<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial); break;
     default: k_observables<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial); break;
