@@ -49,6 +49,11 @@ WORKLOAD = "GLAC gradient flow 32^3x64, beta=6.2, eps=0.01, FP32 links + FP64 su
 STAGE_BYTES_FP32 = (8 * 72 + 4 * 32, 8 * 72 + 8 * 32, 8 * 72 + 4 * 32)
 STAGE_BYTES_FP64 = tuple(2 * b for b in STAGE_BYTES_FP32)
 NCU_TRAFFIC_STAGE0_FP32 = 669986048 + 876275456  # bytes, one ncu capture (see roofline below)
+# FP32 floating-point operations per site of one stage-0 launch: 4 links x
+# (2 x FFMA + FADD + FMUL) thread instructions counted by ncu
+# (sm__sass_thread_inst_executed_op_{ffma,fadd,fmul}_pred_on) on the 32^3x64 launch
+FLOPS_PER_SITE_STAGE0_FP32 = 4 * (2 * 1546 + 41)
+SM_COUNT, FP32_LANES_PER_SM = 148, 128
 
 
 def load_peaks():
@@ -268,6 +273,14 @@ def run_gpu(args):
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind,
                 "stage_ms": [round(x * 1e3, 4) for x in st],
                 "binding_unit": "FP32 FMA pipe (50 % busy per ncu; HBM 22 %)"}
+    # the binding unit: FP32 FLOP/s of the same launch against the FP32 peak at the
+    # median SM clock sampled during the timed region (148 SMs x 128 lanes x 2 FLOP per FMA)
+    sm_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    fp32_peak = SM_COUNT * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
+    fp32_ach = FLOPS_PER_SITE_STAGE0_FP32 * V / float(st[0]) / 1e12
+    roofline["fp32_pipe"] = {"achieved": round(fp32_ach, 2), "peak": round(fp32_peak, 2), "unit": "TFLOP/s",
+                             "frac": round(fp32_ach / fp32_peak, 4), "flops_per_site": FLOPS_PER_SITE_STAGE0_FP32,
+                             "peak_basis": f"148 SMs x 128 FP32 lanes x 2 FLOP x {sm_mhz:.0f} MHz (median under load)"}
 
     # FP64 flow for comparison (same field)
     L64 = g.Lattice(DIMS, beta=BETA, precision="fp64", flow_eps=FLOW_EPS, seed=1, stream_id=rank, device=local)
