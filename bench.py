@@ -435,6 +435,31 @@ def run_profile(args):
     import torch
     import glac_b200 as g
     dims = tuple(int(x) for x in args.dims.split(","))
+    if args.profile == "mlp":
+        # batched spread inference (the warp routine, or --tune 1 for tcgen05 tiles) over 2M feature rows
+        import torch
+        from glac_b200 import learned as lp
+        n = 1 << 21
+        rng = np.random.default_rng(6)
+        X = torch.from_numpy(rng.standard_normal((n, 8)).astype(np.float32)).cuda()
+        P = np.zeros(g.MLP_NPARAMS, np.float32)
+        P[:256] = rng.standard_normal(256) * 0.5
+        P[288:1312] = rng.standard_normal(1024) * 0.25
+        P[1344:1376] = rng.standard_normal(32) * 0.3
+        with lp.ProposalNet() as net:
+            net.params = P
+            net.set_forward_mode(int(args.tune or 0))
+            for _ in range(max(args.steps, 1)):
+                net.forward(X, 0.03, 0.9)
+            if args.time_reps:
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                for _ in range(args.time_reps):
+                    net.forward(X, 0.03, 0.9)
+                sec = (time.perf_counter() - t0) / args.time_reps
+                print(json.dumps({"profile": "mlp", "rows": n, "mode": int(args.tune or 0), "ms": sec * 1e3,
+                                  "rows_per_s": n / sec, "tflops": n * 2 * (16 * 32 + 32 * 32 + 32 * 16) / sec / 1e12}))
+        return
     if args.profile == "ensemble":
         # the seeded uneven ensemble, args.steps sweeps + args.steps flow steps eagerly
         from glac_b200 import ensemble as en
@@ -494,7 +519,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-lattice ensemble leg")
-    ap.add_argument("--profile", choices=["flow", "metropolis", "learned", "ensemble"],
+    ap.add_argument("--profile", choices=["flow", "metropolis", "learned", "ensemble", "mlp"],
                     help="small workload for ncu / variant timing")
     ap.add_argument("--ensemble-n", type=int, default=16, help="lattices in the ensemble profile")
     ap.add_argument("--dims", default="32,32,32,64")

@@ -99,6 +99,222 @@ void launch_mlp_forward(const uint32_t *pack, const float *features, long long n
 }
 
 // ---------------------------------------------------------------------------
+// Batched inference on the 5th-generation tensor cores (tcgen05, TMEM).
+// A CTA of 4 warps takes 128 rows per tile.  Each layer is one or two
+// tcgen05.mma.kind::f16 (M = 128, K = 16; BF16 A and B from shared memory,
+// FP32 accumulator in tensor memory), issued by one thread and completed
+// through an mbarrier; each warp then reads its 32 rows back (tcgen05.ld
+// 32x32b), applies bias and activation, and writes the next layer's operand.
+// Shared-memory operands use the canonical K-major layout without swizzle:
+// 8-row x 16-byte core matrices, rows 16 B apart, 8-row groups SBO = 128 B
+// apart, 16-byte K chunks LBO = rows x 16 B apart.  Rounding points are those
+// of the warp-level path: BF16 inputs, weights, first-layer bias and
+// activations, FP32 accumulation, FP32 b2 and b3.
+// ---------------------------------------------------------------------------
+namespace tcf {
+constexpr int kA1 = 0;         // 128 x 16 BF16 (features, 1, zeros): 4096 B
+constexpr int kA2 = 4096;      // 128 x 32: 8192 B
+constexpr int kA3 = 12288;     // 128 x 32: 8192 B
+constexpr int kB1 = 20480;     // W1^T with b1: 32 x 16: 1024 B
+constexpr int kB2 = 21504;     // W2^T: 32 x 32: 2048 B
+constexpr int kB3 = 23552;     // W3^T padded: 16 x 32: 1024 B
+constexpr int kBar = 24576;    // mbarrier
+constexpr int kSlot = 24584;   // TMEM base address written by tcgen05.alloc
+constexpr int kSmem = 61440;   // requested, so that at most 3 CTAs (3 x 128 TMEM columns) share an SM
+constexpr int kCols = 128;     // TMEM columns: D1 0-31, D2 32-63, D3 64-79
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+// byte offset of BF16 element (row, k) in a K-major, no-swizzle operand of `rows` rows
+__device__ __forceinline__ uint32_t kmaj(int row, int k, int rows) {
+    return (uint32_t)((row & 7) * 16 + (row >> 3) * 128 + (k >> 3) * rows * 16 + (k & 7) * 2);
+}
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, int rows) {
+    const uint64_t lbo = (uint64_t)(rows * 16) >> 4, sbo = 128 >> 4;
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+// kind::f16 instruction descriptor: FP32 D, BF16 A and B, both K-major, M = 128
+__host__ __device__ constexpr uint32_t idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void mma(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t id, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(dtmem), "l"(a), "l"(b), "r"(id), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+// bounded wait for the mbarrier phase; false on timeout
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t phase) {
+    for (uint32_t it = 0; it < kWaitLimit; it++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(bar), "r"(phase)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// 32 lanes x 32 columns: this thread's row, columns col .. col+31
+__device__ __forceinline__ void ld32(uint32_t taddr, float v[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
+}
+}  // namespace tcf
+
+__global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict__ P, const float *__restrict__ feat,
+                                                        long long n, float eps_min, float eps_max,
+                                                        float *__restrict__ eps_out, int *__restrict__ err) {
+    using namespace tcf;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(sm + kSlot);
+    __nv_bfloat16 *s16 = reinterpret_cast<__nv_bfloat16 *>(sm);
+    auto put = [&](int base, int row, int k, int rows, float v) {
+        s16[(base + (int)kmaj(row, k, rows)) >> 1] = __float2bfloat16_rn(v);
+    };
+    // weights (B operands, [n][k] = W[k][n]) once per CTA
+    for (int e = tid; e < 32 * 16; e += 128) {
+        const int nn = e >> 4, k = e & 15;
+        put(kB1, nn, k, 32, k < 8 ? P[kMlpW1 + k * 32 + nn] : (k == 8 ? P[kMlpB1 + nn] : 0.f));
+    }
+    for (int e = tid; e < 32 * 32; e += 128) {
+        const int nn = e >> 5, k = e & 31;
+        put(kB2, nn, k, 32, P[kMlpW2 + k * 32 + nn]);
+    }
+    for (int e = tid; e < 16 * 32; e += 128) {
+        const int nn = e >> 5, k = e & 31;
+        put(kB3, nn, k, 16, nn == 0 ? P[kMlpW3 + k] : 0.f);
+    }
+    const float b3 = P[kMlpB3];
+    const uint32_t bar = sbase + kBar;
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kSlot),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *slot;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    uint32_t phase = 0;
+    bool ok = true;
+    const long long tiles = (n + 127) / 128;
+    // this thread's feature row of a tile (zeros past the end)
+    auto fetch = [&](long long tile, float4 &a, float4 &b) {
+        const long long r = tile * 128 + tid;
+        if (tile < tiles && r < n) {
+            a = __ldg(reinterpret_cast<const float4 *>(feat + r * 8));
+            b = __ldg(reinterpret_cast<const float4 *>(feat + r * 8 + 4));
+        } else {
+            a = make_float4(0.f, 0.f, 0.f, 0.f);
+            b = a;
+        }
+    };
+    float4 fa, fb;
+    fetch(blockIdx.x, fa, fb);
+    for (long long tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const long long row = tile * 128 + tid;
+        const float f[8] = {fa.x, fa.y, fa.z, fa.w, fb.x, fb.y, fb.z, fb.w};
+        fetch(tile + gridDim.x, fa, fb);  // the next tile's row loads while this tile's layers run
+        {
+            uint4 c0, c1;
+            c0.x = pack_bf16(f[0], f[1]); c0.y = pack_bf16(f[2], f[3]);
+            c0.z = pack_bf16(f[4], f[5]); c0.w = pack_bf16(f[6], f[7]);
+            c1.x = pack_bf16(1.f, 0.f); c1.y = 0u; c1.z = 0u; c1.w = 0u;
+            *reinterpret_cast<uint4 *>(sm + kA1 + kmaj(tid, 0, 128)) = c0;
+            *reinterpret_cast<uint4 *>(sm + kA1 + kmaj(tid, 8, 128)) = c1;
+        }
+        float h[32];
+        // three layers: (A, K steps, B, B rows, D column, N)
+        for (int layer = 0; layer < 3 && ok; layer++) {
+            fence_async_smem();
+            fence_before();
+            __syncthreads();
+            fence_after();
+            const int A = layer == 0 ? kA1 : (layer == 1 ? kA2 : kA3);
+            const int B = layer == 0 ? kB1 : (layer == 1 ? kB2 : kB3);
+            const int brows = layer == 2 ? 16 : 32, N = layer == 2 ? 16 : 32, ksteps = layer == 0 ? 1 : 2;
+            const uint32_t dcol = 32u * (uint32_t)layer;
+            if (tid == 0) {
+                for (int ks = 0; ks < ksteps; ks++)
+                    mma(tmem + dcol, sdesc(sbase + A + ks * 2 * 128 * 16, 128),
+                        sdesc(sbase + B + ks * 2 * brows * 16, brows), idesc(N), ks > 0 ? 1u : 0u);
+                commit(bar);
+            }
+            // every thread takes the same branch, so no barrier below is skipped by some threads only
+            ok = __syncthreads_and(wait_phase(bar, phase)) != 0;
+            phase ^= 1u;
+            fence_after();
+            if (!ok) break;
+            ld32(lane_base + dcol, h);
+            if (layer < 2) {
+                const int Anext = layer == 0 ? kA2 : kA3;
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    float v[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const float x = layer == 1 ? h[8 * c + k] + P[kMlpB2 + 8 * c + k] : h[8 * c + k];
+                        v[k] = leaky(x);
+                    }
+                    uint4 w;
+                    w.x = pack_bf16(v[0], v[1]); w.y = pack_bf16(v[2], v[3]);
+                    w.z = pack_bf16(v[4], v[5]); w.w = pack_bf16(v[6], v[7]);
+                    *reinterpret_cast<uint4 *>(sm + Anext + kmaj(tid, 8 * c, 128)) = w;
+                }
+            } else if (row < n) {
+                eps_out[row] = spread_of(h[0] + b3, eps_min, eps_max);
+            }
+        }
+    }
+    if (!ok && err) atomicExch(err, 1);
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+}
+
+void launch_mlp_forward_tc(const float *params, const float *features, long long n, float eps_min, float eps_max,
+                           float *eps_out, int *err, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf::kSmem);
+        attr = true;
+    }
+    const long long tiles = (n + 127) / 128;
+    const int grid = (int)(tiles < 3 * 148 ? tiles : 3 * 148);
+    k_mlp_forward_tc<<<grid, 128, tcf::kSmem, st>>>(params, features, n, eps_min, eps_max, eps_out, err);
+}
+
+// ---------------------------------------------------------------------------
 // Loss and gradient
 // ---------------------------------------------------------------------------
 // J_i(eps) linear between grid points; returns J and its slope.
@@ -364,6 +580,8 @@ struct glac_mlp {
     float *partial = nullptr;
     size_t partial_cap = 0;
     uint32_t *pack = nullptr;
+    int *err_dev = nullptr;  // wait-timeout flag of the tcgen05 kernel
+    int forward_mode = 0;    // 0: the sampler's warp-level routine, 1: tcgen05 tiles
     int step = 0;
     std::string err;
 };
@@ -461,7 +679,7 @@ void glac_mlp_destroy(glac_mlp *M) {
     cudaSetDevice(M->device);
     if (M->stream) cudaStreamSynchronize(M->stream);
     for (void *p : {(void *)M->params, (void *)M->m, (void *)M->v, (void *)M->grad, (void *)M->loss, (void *)M->grid,
-                    (void *)M->partial, (void *)M->pack})
+                    (void *)M->partial, (void *)M->pack, (void *)M->err_dev})
         if (p) cudaFree(p);
     if (M->stream) cudaStreamDestroy(M->stream);
     delete M;
@@ -520,11 +738,32 @@ glac_status glac_mlp_forward(glac_mlp *M, const float *dev_features, long long n
                              float *dev_eps) {
     if (!dev_features || !dev_eps || n <= 0 || !(eps_min < eps_max)) return GLAC_ERR_ARG;
     return mlp_guarded(M, [&] {
-        launch_mlp_forward(M->pack, dev_features, n, (float)eps_min, (float)eps_max, dev_eps, M->stream);
-        mck(cudaGetLastError(), "forward");
+        if (M->forward_mode == 0) {
+            launch_mlp_forward(M->pack, dev_features, n, (float)eps_min, (float)eps_max, dev_eps, M->stream);
+            mck(cudaGetLastError(), "forward");
+            mck(cudaStreamSynchronize(M->stream), "sync");
+            return GLAC_OK;
+        }
+        if (!M->err_dev) mck(cudaMalloc(&M->err_dev, sizeof(int)), "alloc");
+        mck(cudaMemsetAsync(M->err_dev, 0, sizeof(int), M->stream), "memset");
+        launch_mlp_forward_tc(M->params, dev_features, n, (float)eps_min, (float)eps_max, dev_eps, M->err_dev,
+                              M->stream);
+        mck(cudaGetLastError(), "forward (tcgen05)");
+        int flag = 0;
+        mck(cudaMemcpyAsync(&flag, M->err_dev, sizeof(int), cudaMemcpyDeviceToHost, M->stream), "D2H");
         mck(cudaStreamSynchronize(M->stream), "sync");
+        if (flag) {
+            M->err = "tensor-core pass did not complete within its wait limit";
+            return GLAC_ERR_TIMEOUT;
+        }
         return GLAC_OK;
     });
+}
+
+glac_status glac_mlp_set_forward_mode(glac_mlp *M, int mode) {
+    if (!M || (mode != 0 && mode != 1)) return GLAC_ERR_ARG;
+    M->forward_mode = mode;
+    return GLAC_OK;
 }
 
 glac_status glac_mlp_loss_grad(glac_mlp *M, const float *dev_features, const float *dev_esj, long long n, int n_eps,

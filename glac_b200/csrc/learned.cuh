@@ -204,6 +204,9 @@ __device__ __forceinline__ float mlp_spread_warp(const float f[8], const Proposa
 void launch_mlp_pack(const float *params, uint32_t *pack, cudaStream_t st);
 void launch_mlp_forward(const uint32_t *pack, const float *features, long long n, float eps_min, float eps_max,
                         float *eps_out, cudaStream_t st);
+// The same inference on tcgen05 tensor cores from the FP32 parameters (128-row tiles); *err set on a wait timeout.
+void launch_mlp_forward_tc(const float *params, const float *features, long long n, float eps_min, float eps_max,
+                           float *eps_out, int *err, cudaStream_t st);
 // Gradient of L = -(1/n) sum_i J_i(eps_i) (J_i piecewise linear on eps_grid)
 // into grad[kMlpParams] and loss[0]; partial: scratch of mlp_grad_scratch(n) floats.
 size_t mlp_grad_scratch(long long n);

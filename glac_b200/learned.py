@@ -91,6 +91,10 @@ class ProposalNet:
             raise ValueError(f"need {MLP_NPARAMS} parameters")
         self._ck(lib().glac_mlp_set_params(self._h, p.ctypes.data))
 
+    def set_forward_mode(self, mode: int):
+        """0: the sampler's warp-level routine (default); 1: tcgen05 tensor-core tiles."""
+        self._ck(lib().glac_mlp_set_forward_mode(self._h, int(mode)))
+
     def forward(self, features, eps_min: float, eps_max: float):
         torch = _torch()
         f = features.contiguous()

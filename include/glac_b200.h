@@ -235,7 +235,13 @@ glac_status glac_mlp_set_params(glac_mlp *mlp, const float *host_params);
 glac_status glac_mlp_get_params(glac_mlp *mlp, float *host_params);
 /* He-normal initialisation from seed with the output bias at spread eps0. */
 glac_status glac_mlp_init(glac_mlp *mlp, uint64_t seed, double eps_min, double eps_max, double eps0);
-/* dev_eps[i] = spread for dev_features[i*8 .. +8], i < n. */
+/* dev_eps[i] = spread for dev_features[i*8 .. +8], i < n.  Mode 0 (default):
+ * the warp-level tensor-core routine the sampler itself runs (mma.m16n8k16 from
+ * registers); mode 1: 128-row tiles on the 5th-generation tensor cores (tcgen05
+ * MMA into tensor memory; GLAC_ERR_TIMEOUT if a completion wait runs out).
+ * Both round at the same points; at this network size mode 0 is the faster
+ * (36.7 vs 84.2 us per 2M rows on B200). */
+glac_status glac_mlp_set_forward_mode(glac_mlp *mlp, int mode);
 glac_status glac_mlp_forward(glac_mlp *mlp, const float *dev_features, long long n, double eps_min, double eps_max,
                              float *dev_eps);
 /* Loss L = -(1/n) sum_i J_i(eps_i), J_i linear between the n_eps grid points

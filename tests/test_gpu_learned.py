@@ -99,17 +99,35 @@ def test_esj_matches_oracle(g, torch, oracle, prec, flips):
         assert abs(esj.mean() - want.mean()) < 0.01 * want.mean()
 
 
-def test_forward_matches_oracle(g, torch, learned):
+@pytest.mark.parametrize("mode,n", [(0, 3000), (1, 3000), (1, 200_000)])
+def test_forward_matches_oracle(g, torch, learned, mode, n):
+    # mode 0: the sampler's warp routine; mode 1: tcgen05 tensor-core tiles of
+    # 128 rows (3000 rows: a partial last tile; 200k rows: several tiles per CTA)
     rng = np.random.default_rng(1)
-    X = rng.standard_normal((3000, 8)).astype(np.float32)
+    X = rng.standard_normal((n, 8)).astype(np.float32)
     P = random_params(2)
     with learned.ProposalNet() as net:
         net.params = P
+        net.set_forward_mode(mode)
         got = net.forward(torch.from_numpy(X).cuda(), 0.03, 0.9).cpu().numpy()
     want = mlp.spread(P, X, f32(0.03)[()], f32(0.9)[()], emulate=True)
     d = np.abs(got - want)
     assert np.median(d) < 1e-5 and d.max() < 5e-3
     assert got.std() > 0.05  # the spread really varies with the features
+
+
+def test_tensor_core_and_warp_inference_agree(g, torch, learned):
+    rng = np.random.default_rng(8)
+    X = torch.from_numpy(rng.standard_normal((50_000, 8)).astype(np.float32)).cuda()
+    with learned.ProposalNet() as net:
+        net.params = random_params(9)
+        net.set_forward_mode(0)
+        a = net.forward(X, 0.03, 0.9).cpu().numpy()
+        net.set_forward_mode(1)
+        b = net.forward(X, 0.03, 0.9).cpu().numpy()
+    # the same rounding points; the two tensor-core paths sum the FP32 products in different orders
+    d = np.abs(a - b)
+    assert np.median(d) < 1e-6 and d.max() < 5e-3
 
 
 def test_gradient_matches_oracle(g, torch, learned):
