@@ -48,11 +48,11 @@ WORKLOAD = "GLAC gradient flow 32^3x64, beta=6.2, eps=0.01, FP32 links + FP64 su
 # reads 4 links + writes 4 links per stage, force written (stage 0), read+written (1), read (2)
 STAGE_BYTES_FP32 = (8 * 72 + 4 * 32, 8 * 72 + 8 * 32, 8 * 72 + 4 * 32)
 STAGE_BYTES_FP64 = tuple(2 * b for b in STAGE_BYTES_FP32)
-NCU_TRAFFIC_STAGE0_FP32 = 669986048 + 876275456  # bytes, one ncu capture (see roofline below)
+NCU_TRAFFIC_STAGE0_FP32 = 698851840 + 955083520  # bytes, one ncu capture of the launch (80-register variant)
 # FP32 floating-point operations per site of one stage-0 launch: 4 links x
 # (2 x FFMA + FADD + FMUL) thread instructions counted by ncu
 # (sm__sass_thread_inst_executed_op_{ffma,fadd,fmul}_pred_on) on the 32^3x64 launch
-FLOPS_PER_SITE_STAGE0_FP32 = 4 * (2 * 1546 + 41)
+FLOPS_PER_SITE_STAGE0_FP32 = 4 * (2 * 1547 + 59 + 95)
 SM_COUNT, FP32_LANES_PER_SM = 148, 128
 
 
@@ -272,7 +272,7 @@ def run_gpu(args):
                 "kernel": "k_flow_stage<float, morningstar, stage 0>",
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind,
                 "stage_ms": [round(x * 1e3, 4) for x in st],
-                "binding_unit": "FP32 FMA pipe (50 % busy per ncu; HBM 22 %)"}
+                "binding_unit": "FP32 FMA pipe (53 % busy per ncu; HBM 25 %)"}
     # the binding unit: FP32 FLOP/s of the same launch against the FP32 peak at the
     # median SM clock sampled during the timed region (148 SMs x 128 lanes x 2 FLOP per FMA)
     sm_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
