@@ -592,17 +592,27 @@ GLAC_OBS_KERNEL(k_observables_r96, __maxnreg__(96))
 
 // out = [plaq, topc, energy, topct[Nt]] with the reference's normalisations
 // (mastersamplertopcxyz.cpp:13-16, :363-383).
+// Per-slice sums by warps (slice t on warp t mod W; lane l adds the partials
+// l, l+32, ..., then a fixed xor-shuffle tree), the slices then in order by one
+// thread: the same operations in the same order every call.
 __device__ __forceinline__ void obs_finalize_body(int Nt, int nb, int V, const double *partial, double *out) {
     __shared__ double sp[1024], se[1024], sq[1024];
-    for (int t = threadIdx.x; t < Nt; t += blockDim.x) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int t = warp; t < Nt; t += nwarps) {
         double a = 0.0, e = 0.0, q = 0.0;
-        for (int k = 0; k < 2 * nb; k++) {
-            const double *pp = partial + 3 * ((size_t)t * 2 * nb + k);
-            a += pp[0];
-            e += pp[1];
-            q += pp[2];
+        const double *pt = partial + 3 * (size_t)t * 2 * nb;
+        for (int k = lane; k < 2 * nb; k += 32) {
+            a += pt[3 * k];
+            e += pt[3 * k + 1];
+            q += pt[3 * k + 2];
         }
-        sp[t] = a; se[t] = e; sq[t] = q;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            e += __shfl_xor_sync(0xffffffffu, e, o);
+            q += __shfl_xor_sync(0xffffffffu, q, o);
+        }
+        if (lane == 0) { sp[t] = a; se[t] = e; sq[t] = q; }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -634,7 +644,7 @@ void launch_observables(const Geom &g, const LinkField<T> &L, const ObsPlan &pla
     case 96: k_observables_r96<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial); break;
     default: k_observables<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial); break;
     }
-    k_obs_finalize<<<1, 256, 0, st>>>(g.N[3], plan.nb, g.V, partial, out);
+    k_obs_finalize<<<1, 1024, 0, st>>>(g.N[3], plan.nb, g.V, partial, out);
 }
 template <typename T>
 __global__ void __launch_bounds__(256) k_observables_density(Geom g, LinkField<T> L, int nb, int Bv, double *partial,
@@ -646,7 +656,7 @@ void launch_observables_density(const Geom &g, const LinkField<T> &L, const ObsP
                                 double *out, double *dq, double *de, cudaStream_t st) {
     if (g.N[3] > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
     k_observables_density<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial, dq, de);
-    k_obs_finalize<<<1, 256, 0, st>>>(g.N[3], plan.nb, g.V, partial, out);
+    k_obs_finalize<<<1, 1024, 0, st>>>(g.N[3], plan.nb, g.V, partial, out);
 }
 template void launch_observables_density<double>(const Geom &, const LinkField<double> &, const ObsPlan &, double *,
                                                  double *, double *, double *, cudaStream_t);
@@ -731,16 +741,24 @@ __global__ void __launch_bounds__(256) k_observables_weinberg(Geom g, LinkField<
 // out = [plaq, topc, energy, weinberg, topct[Nt], weinbergt[Nt]]
 __global__ void k_weinberg_finalize(int Nt, int nb, int V, const double *partial, double *out) {
     __shared__ double sp[1024], se[1024], sq[1024], sw[1024];
-    for (int t = threadIdx.x; t < Nt; t += blockDim.x) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int t = warp; t < Nt; t += nwarps) {
         double a = 0.0, e = 0.0, q = 0.0, w = 0.0;
-        for (int k = 0; k < 2 * nb; k++) {
-            const double *pp = partial + 4 * ((size_t)t * 2 * nb + k);
-            a += pp[0];
-            e += pp[1];
-            q += pp[2];
-            w += pp[3];
+        const double *pt = partial + 4 * (size_t)t * 2 * nb;
+        for (int k = lane; k < 2 * nb; k += 32) {
+            a += pt[4 * k];
+            e += pt[4 * k + 1];
+            q += pt[4 * k + 2];
+            w += pt[4 * k + 3];
         }
-        sp[t] = a; se[t] = e; sq[t] = q; sw[t] = w;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            e += __shfl_xor_sync(0xffffffffu, e, o);
+            q += __shfl_xor_sync(0xffffffffu, q, o);
+            w += __shfl_xor_sync(0xffffffffu, w, o);
+        }
+        if (lane == 0) { sp[t] = a; se[t] = e; sq[t] = q; sw[t] = w; }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -763,7 +781,7 @@ void launch_weinberg(const Geom &g, const LinkField<T> &L, const ObsPlan &plan, 
                      cudaStream_t st) {
     if (g.N[3] > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
     k_observables_weinberg<T><<<plan.nblocks, plan.B, 0, st>>>(g, L, plan.nb, plan.Bv, partial4);
-    k_weinberg_finalize<<<1, 256, 0, st>>>(g.N[3], plan.nb, g.V, partial4, out);
+    k_weinberg_finalize<<<1, 1024, 0, st>>>(g.N[3], plan.nb, g.V, partial4, out);
 }
 template void launch_weinberg<double>(const Geom &, const LinkField<double> &, const ObsPlan &, double *, double *,
                                       cudaStream_t);
@@ -1256,7 +1274,7 @@ void launch_ens_observables(const LatSlot<T> *slots, const int *start, int nbloc
                             int variant, cudaStream_t st) {
     (void)variant;
     kb_observables<T><<<nblocks, 128, 0, st>>>(slots, start, M, fsel);
-    kb_obs_finalize<T><<<M, 256, 0, st>>>(slots, meas);
+    kb_obs_finalize<T><<<M, 1024, 0, st>>>(slots, meas);
 }
 
 __global__ void k_advance(uint32_t *counter, uint32_t by) { counter[0] += by; }
