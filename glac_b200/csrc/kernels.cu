@@ -160,6 +160,26 @@ template <> __device__ __forceinline__ float su_scalar<float>(double v) { return
 
 GLAC_HD double u_sym16(uint32_t h) { return ((double)h + 0.5) * (1.0 / 65536.0) - 0.5; }
 
+// The same uniform for the FP32 path without a conversion instruction: 2^23 + h
+// read from its bit pattern, minus 2^23, gives h exactly; (h + 1/2) 2^-16 - 1/2
+// = (2h + 1 - 2^16) 2^-17 has at most 17 significant bits, so the FMA is exact
+// and the value equals u_sym16's bit for bit.
+__device__ __forceinline__ float u_sym16f(uint32_t h) {
+    const float hf = __uint_as_float(0x4B000000u | h) - 8388608.f;
+    return __fmaf_rn(hf, 1.f / 65536.f, 0.5f / 65536.f - 0.5f);
+}
+template <typename T> __device__ __forceinline__ T proposal_uniform(uint32_t h);
+template <> __device__ __forceinline__ double proposal_uniform<double>(uint32_t h) { return u_sym16(h); }
+template <> __device__ __forceinline__ float proposal_uniform<float>(uint32_t h) { return u_sym16f(h); }
+
+// Accept uniform in [0, 1): 53 bits for FP64; for FP32 the 23 high bits of word 6
+// as the mantissa of a float in [1, 2), minus 1 (no conversion instruction).
+template <typename T> __device__ __forceinline__ T accept_uniform(uint32_t w6, uint32_t w7);
+template <> __device__ __forceinline__ double accept_uniform<double>(uint32_t w6, uint32_t w7) { return u_53(w6, w7); }
+template <> __device__ __forceinline__ float accept_uniform<float>(uint32_t w6, uint32_t) {
+    return __uint_as_float(0x3F800000u | (w6 >> 9)) - 1.f;
+}
+
 template <typename T>
 __device__ __forceinline__ void su2_near_unity(T u0, T u1, T u2, T u3, T eps, T sq1me, bool flips, T out[4]) {
     // x0 = sign(u0) sqrt(1 - eps^2), x = eps u / |u|, normalised
@@ -169,6 +189,17 @@ __device__ __forceinline__ void su2_near_unity(T u0, T u1, T u2, T u3, T eps, T 
     T x1 = u1 / rn, x2 = u2 / rn, x3 = u3 / rn;
     T nrm = sqrt(x0 * x0 + x1 * x1 + x2 * x2 + x3 * x3);
     out[0] = x0 / nrm; out[1] = x1 / nrm; out[2] = x2 / nrm; out[3] = x3 / nrm;
+}
+// FP32: the same construction with reciprocal square roots in place of the
+// square roots and divisions (which load the special-function pipe).
+template <>
+__device__ __forceinline__ void su2_near_unity<float>(float u0, float u1, float u2, float u3, float eps, float sq1me,
+                                                      bool flips, float out[4]) {
+    const float x0 = (flips && u0 < 0.f) ? -sq1me : sq1me;
+    const float sc = eps * rsqrtf(u1 * u1 + u2 * u2 + u3 * u3);
+    const float x1 = u1 * sc, x2 = u2 * sc, x3 = u3 * sc;
+    const float inv = rsqrtf(x0 * x0 + x1 * x1 + x2 * x2 + x3 * x3);
+    out[0] = x0 * inv; out[1] = x1 * inv; out[2] = x2 * inv; out[3] = x3 * inv;
 }
 
 // X = R S T with the SU(2) elements [[x0 + i x3, x2 + i x1], [-x2 + i x1, x0 - i x3]]
@@ -196,7 +227,7 @@ __device__ __forceinline__ M3<T> rst_matrix(const T r[4], const T s[4], const T 
 template <typename T>
 __device__ __forceinline__ void draw_proposal(uint32_t k0, uint32_t k1, uint32_t link_id, uint32_t sweep,
                                               uint32_t stream_id, int hit, T eps, T sq1me, bool flips, M3<T> &X,
-                                              double &r) {
+                                              T &r) {
     uint32_t w[8];
 #pragma unroll
     for (int call = 0; call < 2; call++) {
@@ -212,17 +243,18 @@ __device__ __forceinline__ void draw_proposal(uint32_t k0, uint32_t k1, uint32_t
         for (int c = 0; c < 4; c++) {
             const int k = 4 * b + c;
             const uint32_t word = w[k >> 1];
-            u[c] = su_scalar<T>(u_sym16((k & 1) ? (word >> 16) : (word & 0xFFFFu)));
+            u[c] = proposal_uniform<T>((k & 1) ? (word >> 16) : (word & 0xFFFFu));
         }
         su2_near_unity<T>(u[0], u[1], u[2], u[3], eps, sq1me, flips, su[b]);
     }
     X = rst_matrix<T>(su[0], su[1], su[2], (w[7] & 1u) == 0u);
-    r = u_53(w[6], w[7]);
+    r = accept_uniform<T>(w[6], w[7]);
 }
 
-template <typename T> __device__ __forceinline__ double accept_weight(T dS);
+// exp(-dS) in the working precision (compared with accept_uniform<T>)
+template <typename T> __device__ __forceinline__ T accept_weight(T dS);
 template <> __device__ __forceinline__ double accept_weight<double>(double dS) { return exp(-dS); }
-template <> __device__ __forceinline__ double accept_weight<float>(float dS) { return (double)expf(-dS); }
+template <> __device__ __forceinline__ float accept_weight<float>(float dS) { return expf(-dS); }
 
 template <typename T>
 __device__ __forceinline__ T delta_s(const M3<T> &U, const M3<T> &Up, const M3<T> &A, T mfac) {
@@ -260,7 +292,7 @@ __device__ __forceinline__ unsigned long long metropolis_hits(const LinkField<T>
 #pragma unroll 1
     for (int h = 0; h < nhits; h++) {
         M3<T> X;
-        double r;
+        T r;
         draw_proposal<T>(k0, k1, link_id, sweep, stream_id, h, eps, sq1me, flips, X, r);
         const T dS = (retr_mul(X, W) - retr(W)) * mfac;
         if (accept_weight<T>(dS) > r) {
@@ -395,7 +427,7 @@ __global__ void __launch_bounds__(128) k_esj(Geom g, LinkField<T> L, float beta,
 #pragma unroll 1
             for (int h = 0; h < nhits; h++) {
                 M3<T> X;
-                double r;
+                T r;
                 draw_proposal<T>(k0, k1, link_id, snapshot, stream_id, h + 16 * (tr + trials * k), eps, sq, flips, X,
                                  r);
                 const T dS = (retr_mul(X, Wc) - retr(Wc)) * mfac;
