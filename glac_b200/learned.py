@@ -247,7 +247,7 @@ def run_chain(start, dims, beta, precision, sweeps, meas_every, flow_eps, flow_s
 
 
 def tau_study(dims=(24, 24, 24, 48), beta=6.0, therm=500, train_sweeps=2000, every=20, stride=64, trials=4,
-              sweeps=5000, meas_every=10, flow_eps=0.02, flow_t=1.0, seed=20261203, steps=3000):
+              sweeps=5000, meas_every=10, flow_eps=0.02, flow_t=1.0, seed=20261203, steps=3000, replicas=1):
     dims = tuple(dims)
     out = dict(dims=list(dims), beta=beta, therm=therm, train_sweeps=train_sweeps, esj_every=every,
                esj_stride=stride, esj_trials=trials, sweeps=sweeps, meas_every=meas_every, flow_eps=flow_eps,
@@ -266,14 +266,26 @@ def tau_study(dims=(24, 24, 24, 48), beta=6.0, therm=500, train_sweeps=2000, eve
     del feat, esj, plain
     out["training"] = rep
     fs = int(round(flow_t / flow_eps))
-    out["chains"] = [
-        run_chain(start, dims, beta, "fp64", sweeps, meas_every, flow_eps, fs, seed + 1, label="plain fp64"),
-        run_chain(start, dims, beta, "fp32", sweeps, meas_every, flow_eps, fs, seed + 2, label="plain fp32"),
-        run_chain(start, dims, beta, "fp32", sweeps, meas_every, flow_eps, fs, seed + 3, su3_eps=rep["best_fixed_eps"],
-                  flips=False, label="fp32 no-flip fixed best eps (ablation)"),
-        run_chain(start, dims, beta, "fp32", sweeps, meas_every, flow_eps, fs, seed + 4, params=params, flips=False,
-                  label="fp32 learned"),
+    kinds = [
+        dict(precision="fp64", label="plain fp64"),
+        dict(precision="fp32", label="plain fp32"),
+        dict(precision="fp32", su3_eps=rep["best_fixed_eps"], flips=False, label="fp32 no-flip fixed best eps (ablation)"),
+        dict(precision="fp32", params=params, flips=False, label="fp32 learned"),
     ]
+    out["replicas"] = replicas
+    out["chains"] = []
+    for ki, kw in enumerate(kinds):
+        runs = [run_chain(start, dims, beta, kw["precision"], sweeps, meas_every, flow_eps, fs,
+                          seed + 1 + 100 * ki + r, **{k: v for k, v in kw.items() if k != "precision"})
+                for r in range(replicas)]
+        c = dict(runs[0])
+        for key in ("wall_s", "acceptance", "plaquette", "tau_int_plaquette", "tau_int_Q", "Q2", "eff_Q_per_s",
+                    "eff_plaq_per_s"):
+            v = np.array([x[key] for x in runs])
+            c[key] = float(v.mean())
+            c[key + "_replica_err"] = float(v.std(ddof=1) / np.sqrt(len(v))) if len(v) > 1 else None
+        c["replica_tau_int_Q"] = [x["tau_int_Q"] for x in runs]
+        out["chains"].append(c)
     base = out["chains"][0]
     for c in out["chains"]:
         c["eff_Q_ratio_vs_plain_fp64"] = c["eff_Q_per_s"] / base["eff_Q_per_s"]
@@ -295,10 +307,11 @@ def _main():
     p.add_argument("--sweeps", type=int, default=5000)
     p.add_argument("--meas-every", type=int, default=10)
     p.add_argument("--steps", type=int, default=3000)
+    p.add_argument("--replicas", type=int, default=1, help="independent chains per sampler")
     p.add_argument("--out", default="")
     a = ap.parse_args()
     r = tau_study(tuple(int(x) for x in a.dims.split(",")), a.beta, a.therm, a.train_sweeps, a.every, a.stride,
-                  sweeps=a.sweeps, meas_every=a.meas_every, steps=a.steps)
+                  sweeps=a.sweeps, meas_every=a.meas_every, steps=a.steps, replicas=a.replicas)
     s = json.dumps(r)
     if a.out:
         with open(a.out, "w") as f:
