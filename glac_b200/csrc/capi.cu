@@ -191,6 +191,10 @@ glac_status glac_create(const glac_desc *desc, glac_ctx **out) {
         V *= d.dims[k];
     }
     if (V > (1ll << 29)) { g_global_err = "lattice too large (V > 2^29)"; return GLAC_ERR_ARG; }
+    if (!field_offsets_fit(V, d.precision == GLAC_FP64)) {
+        g_global_err = "lattice too large for 32-bit field offsets (FP64: V < 1.19e8, FP32: V < 2.68e8 sites)";
+        return GLAC_ERR_ARG;
+    }
     if (d.precision != GLAC_FP64 && d.precision != GLAC_FP32) { g_global_err = "bad precision"; return GLAC_ERR_ARG; }
     if (d.exp_func < 0 || d.exp_func > 3) { g_global_err = "bad exp_func"; return GLAC_ERR_ARG; }
     if (d.n_updates < 0) { g_global_err = "n_updates must be >= 0"; return GLAC_ERR_ARG; }

@@ -300,6 +300,10 @@ glac_status glac_ensemble_create(int n, const int *dims, const double *betas, co
             g_ens_err = "lattice " + std::to_string(i) + ": V <= 2^29 and Nt <= 1024";
             return GLAC_ERR_ARG;
         }
+        if (!field_offsets_fit(V, common->precision == GLAC_FP64)) {
+            g_ens_err = "lattice " + std::to_string(i) + ": too large for 32-bit field offsets";
+            return GLAC_ERR_ARG;
+        }
     }
     glac_ensemble *E = new glac_ensemble;
     E->d = *common;

@@ -125,13 +125,21 @@ GLAC_HD int parity_of_lex(const Geom &g, int lex) {
 // ---------------------------------------------------------------------------
 GLAC_HD int round32(int v) { return (v + 31) & ~31; }
 
+// Element offsets inside a field are 32-bit (fewer address instructions per
+// neighbour load); glac_create and glac_ensemble_create reject lattices whose
+// fields would need more (field_offsets_fit).
+inline bool field_offsets_fit(long long V, bool fp64) {
+    const long long vh32 = ((V / 2) + 31) / 32 * 32;
+    return (fp64 ? 72 : 32) * vh32 < (1ll << 32);
+}
+
 template <typename T> struct LinkField;
 
 template <> struct LinkField<double> {
     double2 *p;
     int Vh, Vh32;
-    GLAC_HD size_t base(int mu, int par, int s) const {
-        return (size_t)(mu * 2 + par) * 9 * (size_t)Vh32 + (size_t)(s >> 5) * 288 + (size_t)(s & 31);
+    GLAC_HD uint32_t base(int mu, int par, int s) const {
+        return (uint32_t)(mu * 2 + par) * (9u * (uint32_t)Vh32) + (uint32_t)(s >> 5) * 288u + (uint32_t)(s & 31);
     }
     __device__ __forceinline__ M3<double> load(int mu, int par, int s) const {
         const double2 *b = p + base(mu, par, s);
@@ -164,10 +172,10 @@ template <> struct LinkField<float> {
     float4 *p4;
     float2 *p2;
     int Vh, Vh32;
-    GLAC_HD size_t base4(int mu, int par, int s) const {
-        return (size_t)(mu * 2 + par) * 4 * (size_t)Vh32 + (size_t)(s >> 5) * 128 + (size_t)(s & 31);
+    GLAC_HD uint32_t base4(int mu, int par, int s) const {
+        return (uint32_t)(mu * 2 + par) * (4u * (uint32_t)Vh32) + (uint32_t)(s >> 5) * 128u + (uint32_t)(s & 31);
     }
-    GLAC_HD size_t at2(int mu, int par, int s) const { return ((size_t)(mu * 2 + par)) * (size_t)Vh + (size_t)s; }
+    GLAC_HD uint32_t at2(int mu, int par, int s) const { return (uint32_t)(mu * 2 + par) * (uint32_t)Vh + (uint32_t)s; }
     __device__ __forceinline__ M3<float> load(int mu, int par, int s) const {
         const float4 *b = p4 + base4(mu, par, s);
         M3<float> U;
@@ -206,8 +214,8 @@ template <typename T> struct ForceField;
 template <> struct ForceField<double> {
     double2 *p;
     int Vh, Vh32;
-    GLAC_HD size_t base(int mu, int par, int s) const {
-        return (size_t)(mu * 2 + par) * 4 * (size_t)Vh32 + (size_t)(s >> 5) * 128 + (size_t)(s & 31);
+    GLAC_HD uint32_t base(int mu, int par, int s) const {
+        return (uint32_t)(mu * 2 + par) * (4u * (uint32_t)Vh32) + (uint32_t)(s >> 5) * 128u + (uint32_t)(s & 31);
     }
     __device__ __forceinline__ AH8<double> load(int mu, int par, int s) const {
         const double2 *b = p + base(mu, par, s);
@@ -229,8 +237,8 @@ template <> struct ForceField<double> {
 template <> struct ForceField<float> {
     float4 *p;
     int Vh, Vh32;
-    GLAC_HD size_t base(int mu, int par, int s) const {
-        return (size_t)(mu * 2 + par) * 2 * (size_t)Vh32 + (size_t)(s >> 5) * 64 + (size_t)(s & 31);
+    GLAC_HD uint32_t base(int mu, int par, int s) const {
+        return (uint32_t)(mu * 2 + par) * (2u * (uint32_t)Vh32) + (uint32_t)(s >> 5) * 64u + (uint32_t)(s & 31);
     }
     __device__ __forceinline__ AH8<float> load(int mu, int par, int s) const {
         const float4 *b = p + base(mu, par, s);

@@ -60,7 +60,11 @@ typedef struct {
 typedef struct glac_ctx glac_ctx;
 
 /* ---- lifetime ---------------------------------------------------------- */
-/* Replaces System::latticeSetup's allocation (GLAC/system.cpp:148-177, 193-231). */
+/* Replaces System::latticeSetup's allocation (GLAC/system.cpp:148-177, 193-231).
+ * Every extent even and >= 4 (checkerboard), Nt <= 1024, and a volume whose
+ * fields fit 32-bit element offsets: V < 1.19e8 sites in FP64, < 2.68e8 in FP32
+ * (beyond what two fields and the force of one lattice leave room for in
+ * 180 GB anyway).  Errors: GLAC_ERR_ARG, message in glac_global_error(). */
 glac_status glac_create(const glac_desc *desc, glac_ctx **out);
 void glac_destroy(glac_ctx *ctx);
 const char *glac_last_error(const glac_ctx *ctx);

@@ -325,3 +325,18 @@ def test_weinberg_matches_reference(g, oracle, reference, prec, tol):
             base = L.measure()
         assert rel_err(got, want) < tol
         assert rel_err(got[[0, 1, 2]], base[:3]) < 1e-13 and rel_err(got[4:12], base[3:]) < 1e-12
+
+
+def test_observables_at_the_largest_time_extent(g, oracle):
+    # Nt = 1024 fills the per-slice arrays of the reduction; larger Nt is rejected at creation
+    N = (4, 4, 4, 1024)
+    links = oracle.haar_field(N, 41)
+    with lattice(g, N, "fp64") as L:
+        L.set_links(links)
+        got = L.measure()
+        assert got.size == 3 + 1024
+        assert rel_err(got, oracle.observables(N, links)) < 1e-12
+        _, q, _ = L.measure_density()
+        assert abs(q.sum() - got[1]) < 1e-9
+    with pytest.raises(g.GlacError):
+        lattice(g, (4, 4, 4, 1026), "fp64")
