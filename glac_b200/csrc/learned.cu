@@ -304,11 +304,8 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
 
 void launch_mlp_forward_tc(const float *params, const float *features, long long n, float eps_min, float eps_max,
                            float *eps_out, int *err, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf::kSmem);
-        attr = true;
-    }
+    // per device (cheap): the attribute is not shared between devices
+    cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf::kSmem);
     const long long tiles = (n + 127) / 128;
     const int grid = (int)(tiles < 3 * 148 ? tiles : 3 * 148);
     k_mlp_forward_tc<<<grid, 128, tcf::kSmem, st>>>(params, features, n, eps_min, eps_max, eps_out, err);
