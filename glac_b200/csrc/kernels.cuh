@@ -18,13 +18,24 @@ __device__ __forceinline__ M3<T> staple(const LinkField<T> &L, const Geom &g, co
     M3<T> A;
     set_zero(A);
     const int q = p ^ 1;
-    const int s_mu = lex_step(g, n, mu, +1) >> 1;
+    // Neighbour indices: select chains in FP32 (pick4), indexed arrays in FP64;
+    // each form is the faster one for its precision.
+    const int f_mu = sizeof(T) == 4 ? step_offset(g, n, mu, +1) : step_offset_indexed(g, n, mu, +1);
+    const int s_mu = (n.lex + f_mu) >> 1;
 #pragma unroll 1
     for (int nu = 0; nu < 4; nu++) {
         if (nu == mu) continue;
-        const int s_nup = lex_step(g, n, nu, +1) >> 1;
-        const int s_num = lex_step(g, n, nu, -1) >> 1;
-        const int s_diag = lex_step2(g, n, mu, +1, nu, -1) >> 1;
+        int s_nup, s_num, s_diag;
+        if constexpr (sizeof(T) == 4) {
+            const int b_nu = step_offset(g, n, nu, -1);
+            s_nup = (n.lex + step_offset(g, n, nu, +1)) >> 1;
+            s_num = (n.lex + b_nu) >> 1;
+            s_diag = (n.lex + f_mu + b_nu) >> 1;
+        } else {
+            s_nup = lex_step(g, n, nu, +1) >> 1;
+            s_num = lex_step(g, n, nu, -1) >> 1;
+            s_diag = lex_step2(g, n, mu, +1, nu, -1) >> 1;
+        }
         {
             M3<T> a = L.load(nu, q, s_mu);
             M3<T> b = L.load(mu, q, s_nup);

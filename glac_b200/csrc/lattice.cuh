@@ -90,23 +90,31 @@ GLAC_HD Site site_from_ps(const Geom &g, int p, int s) {
     return st;
 }
 
-// lexicographic index of n + a e_d (a = +1 or -1), periodic
-GLAC_HD int lex_step(const Geom &g, const Site &n, int d, int a) {
-    int cd = n.c[d];
-    int off;
-    if (a > 0) off = (cd == g.N[d] - 1) ? -(g.N[d] - 1) * g.stride[d] : g.stride[d];
-    else off = (cd == 0) ? (g.N[d] - 1) * g.stride[d] : -g.stride[d];
-    return n.lex + off;
+// periodic offset of one step a = +1 or -1 along d, by indexing the arrays
+GLAC_HD int step_offset_indexed(const Geom &g, const Site &n, int d, int a) {
+    const int cd = n.c[d];
+    if (a > 0) return (cd == g.N[d] - 1) ? -(g.N[d] - 1) * g.stride[d] : g.stride[d];
+    return (cd == 0) ? (g.N[d] - 1) * g.stride[d] : -g.stride[d];
 }
+// lexicographic index of n + a e_d (a = +1 or -1), periodic
+GLAC_HD int lex_step(const Geom &g, const Site &n, int d, int a) { return n.lex + step_offset_indexed(g, n, d, a); }
 // lexicographic index of n + a e_d + b e_e (d != e)
 GLAC_HD int lex_step2(const Geom &g, const Site &n, int d, int a, int e, int b) {
-    int cd = n.c[d], ce = n.c[e];
-    int off;
-    if (a > 0) off = (cd == g.N[d] - 1) ? -(g.N[d] - 1) * g.stride[d] : g.stride[d];
-    else off = (cd == 0) ? (g.N[d] - 1) * g.stride[d] : -g.stride[d];
-    if (b > 0) off += (ce == g.N[e] - 1) ? -(g.N[e] - 1) * g.stride[e] : g.stride[e];
-    else off += (ce == 0) ? (g.N[e] - 1) * g.stride[e] : -g.stride[e];
-    return n.lex + off;
+    return n.lex + step_offset_indexed(g, n, d, a) + step_offset_indexed(g, n, e, b);
+}
+
+// v[d] for a direction d that may be a run-time value, as a chain of selects:
+// the arrays stay in registers, where indexing them with a run-time d places
+// the Site and the Geom in local memory.  Folds to v[d] for a constant d.  The
+// FP32 staple (flow stage, Metropolis) runs faster with it; the FP64 staple and
+// the clover run faster with the indexed form above (timed on B200 at 32^3 x 64).
+GLAC_HD int pick4(const int v[4], int d) { return d == 0 ? v[0] : d == 1 ? v[1] : d == 2 ? v[2] : v[3]; }
+
+// periodic offset of one step a = +1 or -1 along d, selected without indexing
+GLAC_HD int step_offset(const Geom &g, const Site &n, int d, int a) {
+    const int cd = pick4(n.c, d), Nd = pick4(g.N, d), sd = pick4(g.stride, d);
+    if (a > 0) return (cd == Nd - 1) ? -(Nd - 1) * sd : sd;
+    return (cd == 0) ? (Nd - 1) * sd : -sd;
 }
 
 GLAC_HD int parity_of_lex(const Geom &g, int lex) {
