@@ -272,7 +272,7 @@ def run_gpu(args):
                 "kernel": "k_flow_stage<float, morningstar, stage 0>",
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind,
                 "stage_ms": [round(x * 1e3, 4) for x in st],
-                "binding_unit": "FP32 FMA pipe (53 % busy per ncu; HBM 25 %)"}
+                "binding_unit": "FP32 FMA pipe (60 % busy per ncu; HBM 25 %)"}
     # the binding unit: FP32 FLOP/s of the same launch against the FP32 peak at the
     # median SM clock sampled during the timed region (148 SMs x 128 lanes x 2 FLOP per FMA)
     sm_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
