@@ -67,12 +67,13 @@ __device__ __forceinline__ void flow_stage_body(const Geom &g, const LinkField<T
 GLAC_FLOW_KERNEL(k_flow_stage, __launch_bounds__(128))
 GLAC_FLOW_KERNEL(k_flow_stage_r128, __maxnreg__(128))
 GLAC_FLOW_KERNEL(k_flow_stage_r80, __maxnreg__(80))
+GLAC_FLOW_KERNEL(k_flow_stage_r96, __maxnreg__(96))
 
 // Launch-bound variants (minimum resident blocks of 128 threads per SM, i.e.
 // the register cap) that the autotuner chooses among; variant 0 is the default.
 // Register caps per variant ([fp64, fp32]; 0 = no cap, -1 = unused slot); the
 // flow family also varies the site-block shape.
-const int kFlowRegs[2][kMaxVariants] = {{0, 128, 0, -1}, {0, 80, 0, -1}};
+const int kFlowRegs[2][kMaxVariants] = {{0, 128, 0, -1}, {0, 80, 0, 96}};
 const int kFlowShape[2][kMaxVariants] = {{0, 0, 1, 0}, {0, 0, 1, 0}};
 const int kMetroRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 96, 80, 128}};
 const int kObsRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 128, 168, -1}};
@@ -103,6 +104,12 @@ static void flow_dispatch(int regs, int shape, cudaStream_t st, const Geom &g, c
     const dim3 grid(8 * ((g.Vh + 127) / 128));
     switch (regs) {
     case 128: k_flow_stage_r128<T, KIND, STAGE, 0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b); break;
+    case 96:
+        if constexpr (sizeof(T) == 4) {
+            k_flow_stage_r96<T, KIND, STAGE, 0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b);
+            break;
+        }
+        [[fallthrough]];
     case 80:
         if constexpr (sizeof(T) == 4) {
             k_flow_stage_r80<T, KIND, STAGE, 0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b);
@@ -1255,6 +1262,7 @@ void launch_ens_metropolis(const LatSlot<T> *slots, const int *start, int nblock
     }
 GLAC_ENS_FLOW_KERNEL(kb_flow_stage, __launch_bounds__(128))
 GLAC_ENS_FLOW_KERNEL(kb_flow_stage_r80, __maxnreg__(80))
+GLAC_ENS_FLOW_KERNEL(kb_flow_stage_r96, __maxnreg__(96))
 GLAC_ENS_FLOW_KERNEL(kb_flow_stage_r128, __maxnreg__(128))
 #undef GLAC_ENS_FLOW_KERNEL
 
@@ -1267,6 +1275,12 @@ static void ens_flow_dispatch(int regs, int shape, int nblocks, cudaStream_t st,
     }
     switch (regs) {
     case 128: kb_flow_stage_r128<T, STAGE, 0><<<nblocks, 128, 0, st>>>(slots, start, M, src, dst, a, b); break;
+    case 96:
+        if constexpr (sizeof(T) == 4) {
+            kb_flow_stage_r96<T, STAGE, 0><<<nblocks, 128, 0, st>>>(slots, start, M, src, dst, a, b);
+            break;
+        }
+        [[fallthrough]];
     case 80:
         if constexpr (sizeof(T) == 4) {
             kb_flow_stage_r80<T, STAGE, 0><<<nblocks, 128, 0, st>>>(slots, start, M, src, dst, a, b);
