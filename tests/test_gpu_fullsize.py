@@ -1,0 +1,103 @@
+"""Properties that hold at any size, checked at the benchmark size 32^3 x 64
+(2,097,152 sites), where the oracle is too slow to compare site by site:
+gauge invariance (the reference's own check, latticeoperations.cpp:750-813),
+covariance under a one-site shift in time (which swaps the parities of every
+site), FP32 against FP64 over a flow, sweeps that compose, per-site densities
+that sum to the global observables, and unitarity after the flow.
+Tolerances: FP64 <= 1e-12 relative, FP32 <= 1e-5 relative on plaquette and E;
+topological charge compared in absolute terms (it is O(1) here)."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from test_oracle import gauge_transform
+
+pytestmark = pytest.mark.gpu
+
+N = (32, 32, 32, 64)
+TOL = {"fp64": 1e-12, "fp32": 1e-5}
+Q_TOL = {"fp64": 1e-9, "fp32": 1e-3}
+
+
+@pytest.fixture(scope="module")
+def g():
+    import glac_b200
+    return glac_b200
+
+
+@pytest.fixture(scope="module")
+def start(g):
+    """A Haar start after 5 FP64 sweeps at beta = 6.2 (host layout, FP64)."""
+    with g.Lattice(N, beta=6.2, precision="fp64", seed=7) as L:
+        L.hot_start(7)
+        L.metropolis(5)
+        return L.get_links()
+
+
+def measured(g, links, prec):
+    with g.Lattice(N, beta=6.2, precision=prec) as L:
+        L.set_links(links)
+        return L.measure()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_gauge_invariance_full_size(g, oracle, start, prec):
+    W = oracle.haar_field(N, 99)[0].copy()
+    a = measured(g, start, prec)
+    b = measured(g, gauge_transform(start, W, N), prec)
+    assert rel_err(b[[0, 2]], a[[0, 2]]) < TOL[prec]
+    assert np.max(np.abs(b[1:2] - a[1:2])) < Q_TOL[prec]
+    assert np.max(np.abs(b[3:] - a[3:])) < Q_TOL[prec]  # q(t) per slice
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_time_shift_covariance_full_size(g, start, prec):
+    # U'(x, t) = U(x, t - 1): every site changes parity; globals stay, q(t) rolls by one slice
+    shifted = np.roll(start.reshape(4, N[3], N[2] * N[1] * N[0], 18), 1, axis=1).reshape(start.shape)
+    a = measured(g, start, prec)
+    b = measured(g, shifted, prec)
+    assert rel_err(b[[0, 2]], a[[0, 2]]) < TOL[prec]
+    assert abs(b[1] - a[1]) < Q_TOL[prec]
+    assert np.max(np.abs(b[3:] - np.roll(a[3:], 1))) < Q_TOL[prec]
+
+
+def test_fp32_flow_tracks_fp64_full_size(g, start):
+    obs = {}
+    for prec in ("fp64", "fp32"):
+        with g.Lattice(N, beta=6.2, precision=prec, flow_eps=0.01) as L:
+            L.set_links(start)
+            obs[prec] = L.flow(20)
+            if prec == "fp32":
+                assert L.unitarity_violation() < 1e-5
+    a, b = obs["fp64"], obs["fp32"]
+    assert a.shape == (21, 3 + N[3])
+    assert rel_err(b[:, [0, 2]], a[:, [0, 2]]) < TOL["fp32"]
+    assert np.max(np.abs(b[:, 1] - a[:, 1])) < Q_TOL["fp32"]
+    assert np.all(np.diff(a[:, 0]) > 0)  # the flow smooths: plaquette rises every step
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_sweeps_compose_full_size(g, start, prec):
+    with g.Lattice(N, beta=6.2, precision=prec, seed=5) as A, g.Lattice(N, beta=6.2, precision=prec, seed=5) as B:
+        A.set_links(start)
+        B.set_links(start)
+        acc_a = A.metropolis(2)
+        acc_b = B.metropolis(1) + B.metropolis(1)
+        assert A.sweep == B.sweep == 2
+        assert np.array_equal(A.get_links(), B.get_links())
+        assert abs(acc_a - acc_b / 2) < 1e-12
+        assert 0.02 < acc_a < 0.8
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_densities_sum_to_globals_full_size(g, start, prec):
+    with g.Lattice(N, beta=6.2, precision=prec) as L:
+        L.set_links(start)
+        obs, q, e = L.measure_density()
+        assert rel_err(obs, L.measure()) < 1e-14
+    assert q.shape == e.shape == (int(np.prod(N)),)
+    assert abs(q.sum() - obs[1]) < 1e-9
+    assert abs(e.sum() / q.size - obs[2]) < 1e-10 * abs(obs[2])
+    # q(t) per slice from the density, lexicographic order with t slowest
+    qt = q.reshape(N[3], -1).sum(axis=1)
+    assert np.max(np.abs(qt - obs[3:])) < 1e-9
