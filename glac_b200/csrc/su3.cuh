@@ -29,6 +29,7 @@ struct Cx {
 template <typename R> GLAC_HD Cx<R> cx(R a, R b) { Cx<R> z; z.re = a; z.im = b; return z; }
 template <typename R> GLAC_HD Cx<R> operator+(Cx<R> a, Cx<R> b) { return cx(a.re + b.re, a.im + b.im); }
 template <typename R> GLAC_HD Cx<R> operator-(Cx<R> a, Cx<R> b) { return cx(a.re - b.re, a.im - b.im); }
+template <typename R> GLAC_HD Cx<R> operator-(Cx<R> a) { return cx(-a.re, -a.im); }
 template <typename R> GLAC_HD Cx<R> conj(Cx<R> a) { return cx(a.re, -a.im); }
 template <typename R> GLAC_HD Cx<R> operator*(Cx<R> a, Cx<R> b) {
     return cx(fmaR(a.re, b.re, -(a.im * b.im)), fmaR(a.re, b.im, a.im * b.re));
@@ -180,6 +181,32 @@ template <typename R> GLAC_HD void acc_mul(M3<R> &Acc, const M3<R> &A, const M3<
             s = cmac(s, A(i, 0), B(0, j));
             s = cmac(s, A(i, 1), B(1, j));
             s = cmac(s, A(i, 2), B(2, j));
+            Acc(i, j) = s;
+        }
+}
+// Acc -= A B
+template <typename R> GLAC_HD void sub_mul(M3<R> &Acc, const M3<R> &A, const M3<R> &B) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            Cx<R> s = Acc(i, j);
+            s = cmac(s, -A(i, 0), B(0, j));
+            s = cmac(s, -A(i, 1), B(1, j));
+            s = cmac(s, -A(i, 2), B(2, j));
+            Acc(i, j) = s;
+        }
+}
+// Acc -= A B^+
+template <typename R> GLAC_HD void sub_mul_nd(M3<R> &Acc, const M3<R> &A, const M3<R> &B) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            Cx<R> s = Acc(i, j);
+            s = cmac_bc(s, -A(i, 0), B(j, 0));
+            s = cmac_bc(s, -A(i, 1), B(j, 1));
+            s = cmac_bc(s, -A(i, 2), B(j, 2));
             Acc(i, j) = s;
         }
 }
