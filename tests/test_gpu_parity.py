@@ -159,6 +159,30 @@ def test_autotune_restores_state_and_keeps_results(g, oracle):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_flow_variants_agree(g, oracle, prec):
+    # (z, t) pairs of two 128-site chunks and Nz, Nt multiples of 4, so the
+    # tiled chunk order really permutes the blocks; every flow variant (register
+    # caps, site-block shapes) must give the same field and observables
+    N = (32, 16, 8, 8)
+    start = oracle.haar_field(N, 31)
+    ref = None
+    for v in range(4):
+        with lattice(g, N, prec) as L:
+            try:
+                L.tuning = [v, 0, 0]
+            except g.GlacError:
+                continue
+            L.set_links(start)
+            obs = L.flow(3)
+            links = L.get_links()
+        if ref is None:
+            ref = (obs, links)
+            assert rel_err(links, oracle.flow(N, start, 0.01, 3)) < TOL[prec]
+        else:
+            assert rel_err(links, ref[1]) < TOL[prec] and rel_err(obs, ref[0]) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_flow_vs_live_reference_larger(g, oracle, reference, prec):
     N = (8, 8, 8, 8)
     reference.configure(8, 8, flow_eps=0.02, nflows=4)
