@@ -532,7 +532,7 @@ glac_status glac_ensemble_set_tuning(glac_ensemble *E, const int *v) {
     if (!E || !v) return GLAC_ERR_ARG;
     const bool fp32 = E->d.precision == GLAC_FP32;
     for (int f = 0; f < 3; f++)
-        if (v[f] < 0 || v[f] >= (f == FAM_OBS ? 1 : num_variants((Family)f, fp32))) {
+        if (v[f] < 0 || v[f] >= num_variants((Family)f, fp32)) {
             E->err = "launch variant out of range";
             return GLAC_ERR_ARG;
         }
@@ -541,10 +541,11 @@ glac_status glac_ensemble_set_tuning(glac_ensemble *E, const int *v) {
     return GLAC_OK;
 }
 
-// Times every launch variant of the Metropolis and flow families on the whole
-// ensemble (in the flow buffers: the chain, its sweep counter and the
+// Times every launch variant of the flow, Metropolis and observable families on
+// the whole ensemble (in the flow buffers: the chain, its sweep counter and the
 // acceptance counters are left as they were) and keeps the fastest.
-// report[4 f + v] = seconds per sweep / per flow step (0 for absent variants).
+// report[4 f + v] = seconds per flow step / per sweep / per measurement (0 for
+// absent variants).
 glac_status glac_ensemble_autotune(glac_ensemble *E, int reps, double *report) {
     return eguarded(E, [&] {
         glac_status s = need_field(E);
@@ -559,7 +560,9 @@ glac_status glac_ensemble_autotune(glac_ensemble *E, int reps, double *report) {
         cudaEvent_t e0, e1;
         eck(cudaEventCreate(&e0), "event");
         eck(cudaEventCreate(&e1), "event");
-        for (int fam = 0; fam < 2; fam++) {
+        // the observable family measures the flow buffer into row 0 of each lattice's
+        // rows (allocated since creation)
+        for (int fam = 0; fam < 3; fam++) {
             const int nv = num_variants((Family)fam, fp32);
             int best = E->tune[fam];
             double best_t = 1e30;
@@ -573,6 +576,9 @@ glac_status glac_ensemble_autotune(glac_ensemble *E, int reps, double *report) {
                         if (fam == FAM_METRO) {
                             if (fp32) sweeps_t<float>(E, 1, 1);
                             else sweeps_t<double>(E, 1, 1);
+                        } else if (fam == FAM_OBS) {
+                            if (fp32) observe_t<float>(E, 1, 0);
+                            else observe_t<double>(E, 1, 0);
                         } else {
                             if (fp32) flow_t<float>(E, 1, false);
                             else flow_t<double>(E, 1, false);

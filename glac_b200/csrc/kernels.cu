@@ -1387,13 +1387,18 @@ void launch_ens_flow_stage(const LatSlot<T> *slots, const int *start, int nblock
     else ens_flow_dispatch<T, 2>(regs, shape, nblocks, st, slots, start, M, src, dst, a, b);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(128) kb_observables(const LatSlot<T> *__restrict__ slots,
-                                                      const int *__restrict__ start, int M, int fsel) {
-    const int i = slot_of(start, M, blockIdx.x);
-    const LatSlot<T> &S = slots[i];
-    observables_body<T>(S.g, S.f[fsel], S.nb, S.Bv, S.partial, blockIdx.x - __ldg(start + i));
-}
+#define GLAC_ENS_OBS_KERNEL(NAME, ATTR)                                                                      \
+    template <typename T>                                                                                  \
+    __global__ void ATTR NAME(const LatSlot<T> *__restrict__ slots, const int *__restrict__ start, int M,    \
+                              int fsel) {                                                                  \
+        const int i = slot_of(start, M, blockIdx.x);                                                       \
+        const LatSlot<T> &S = slots[i];                                                                    \
+        observables_body<T>(S.g, S.f[fsel], S.nb, S.Bv, S.partial, blockIdx.x - __ldg(start + i));          \
+    }
+GLAC_ENS_OBS_KERNEL(kb_observables, __launch_bounds__(128))
+GLAC_ENS_OBS_KERNEL(kb_observables_r128, __maxnreg__(128))
+GLAC_ENS_OBS_KERNEL(kb_observables_r168, __maxnreg__(168))
+#undef GLAC_ENS_OBS_KERNEL
 template <typename T>
 __global__ void kb_obs_finalize(const LatSlot<T> *__restrict__ slots, int meas) {
     const LatSlot<T> &S = slots[blockIdx.x];
@@ -1402,8 +1407,16 @@ __global__ void kb_obs_finalize(const LatSlot<T> *__restrict__ slots, int meas) 
 template <typename T>
 void launch_ens_observables(const LatSlot<T> *slots, const int *start, int nblocks, int M, int fsel, int meas,
                             int variant, cudaStream_t st) {
-    (void)variant;
-    kb_observables<T><<<nblocks, 128, 0, st>>>(slots, start, M, fsel);
+    switch (variant_regs(FAM_OBS, sizeof(T) == 4, variant)) {
+    case 128: kb_observables_r128<T><<<nblocks, 128, 0, st>>>(slots, start, M, fsel); break;
+    case 168:
+        if constexpr (sizeof(T) == 4) {
+            kb_observables_r168<T><<<nblocks, 128, 0, st>>>(slots, start, M, fsel);
+            break;
+        }
+        [[fallthrough]];  // no 168-register FP64 variant
+    default: kb_observables<T><<<nblocks, 128, 0, st>>>(slots, start, M, fsel); break;
+    }
     kb_obs_finalize<T><<<M, 1024, 0, st>>>(slots, meas);
 }
 

@@ -171,7 +171,8 @@ class Ensemble:
     def autotune(self, reps=2):
         rep = np.zeros(12)
         self._ck(lib().glac_ensemble_autotune(self._h, int(reps), rep.ctypes.data))
-        return {"flow": rep[0:4].tolist(), "metropolis": rep[4:8].tolist(), "chosen": self.tuning}
+        return {"flow": rep[0:4].tolist(), "metropolis": rep[4:8].tolist(), "observables": rep[8:12].tolist(),
+                "chosen": self.tuning}
 
     @property
     def tuning(self):

@@ -298,8 +298,10 @@ glac_status glac_ensemble_flow(glac_ensemble *ens, int n_steps, double *obs);
 glac_status glac_ensemble_run(glac_ensemble *ens, int n_sweeps, int n_steps, double *acceptance, double *obs,
                               double *gpu_seconds);
 /* Launch-variant autotuner over the whole ensemble (flow site-block shapes and
- * register caps, Metropolis register caps); report[4 f + v] = seconds per
- * flow step (f = 0) / per sweep (f = 1) of variant v.  Leaves the chains as they were. */
+ * register caps, Metropolis and observable register caps); report[4 f + v] =
+ * seconds per flow step (f = 0) / per sweep (f = 1) / per measurement (f = 2)
+ * of variant v.  Leaves the chains as they were (a measurement row written
+ * while timing is overwritten by the next run). */
 glac_status glac_ensemble_autotune(glac_ensemble *ens, int reps, double *report);
 glac_status glac_ensemble_get_tuning(const glac_ensemble *ens, int *variants3);
 glac_status glac_ensemble_set_tuning(glac_ensemble *ens, const int *variants3);

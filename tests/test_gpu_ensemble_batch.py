@@ -81,9 +81,21 @@ def test_autotune_leaves_chains_alone(g, ens):
         E.metropolis(1)
         F.metropolis(1)
         rep = E.autotune(1)
-        assert rep["flow"][0] > 0 and rep["metropolis"][0] > 0
+        assert rep["flow"][0] > 0 and rep["metropolis"][0] > 0 and rep["observables"][0] > 0
         for i in range(len(DIMS)):
             assert np.array_equal(E.get_links(i), F.get_links(i))
+        # every observable variant measures the same flowed fields
+        chosen = E.tuning
+        base = None
+        for v in range(3):
+            E.tuning = [0, 0, v]
+            obs = E.flow(2)
+            if base is None:
+                base = obs
+            else:
+                for i in range(len(DIMS)):
+                    assert rel(obs[i], base[i]) < 1e-5
+        E.tuning = chosen
         # every variant computes the same chain
         a, b = E.metropolis(2), F.metropolis(2)
         assert np.allclose(a, b, atol=0.01)
