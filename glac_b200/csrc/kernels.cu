@@ -363,7 +363,7 @@ __device__ __forceinline__ void metropolis_body(const Geom &g, const LinkField<T
         Site n;
         if (valid) {
             n = site_from_ps(g, p, s);
-            A = staple(L, g, n, p, mu);
+            A = staple<T, true>(L, g, n, p, mu);
             staple_features(A, beta, f);
         }
         const float e = mlp_spread_warp(f, P, feat + (threadIdx.x >> 5) * 128);
@@ -374,7 +374,7 @@ __device__ __forceinline__ void metropolis_body(const Geom &g, const LinkField<T
         }
     } else if (valid) {
         const Site n = site_from_ps(g, p, s);
-        const M3<T> A = staple(L, g, n, p, mu);
+        const M3<T> A = staple<T, true>(L, g, n, p, mu);
         na = metropolis_hits<T>(L, mu, p, s, A, mfac, eps, sq1me, P.flips, nhits, k0, k1,
                                 (uint32_t)mu * (uint32_t)g.V + (uint32_t)n.lex, sweep, stream_id);
     }

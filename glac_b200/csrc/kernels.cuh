@@ -13,7 +13,9 @@ namespace glac {
 // getActionDerivative :55-86):
 //   sum_{nu != mu}  U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+  +  U_nu(n+mu-nu)^+ U_mu(n-nu)^+ U_nu(n-nu)
 // n has parity p; n +- nu and n + mu have parity 1-p, n + mu - nu has parity p.
-template <typename T>
+// UNROLL: the nu loop unrolled, which made the Metropolis sub-sweep 1-4 % faster
+// and the flow stage 2-6 % slower on B200 (the flow keeps the rolled loop).
+template <typename T, bool UNROLL = false>
 __device__ __forceinline__ M3<T> staple(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu) {
     M3<T> A;
     set_zero(A);
@@ -22,7 +24,7 @@ __device__ __forceinline__ M3<T> staple(const LinkField<T> &L, const Geom &g, co
     // each form is the faster one for its precision.
     const int f_mu = sizeof(T) == 4 ? step_offset(g, n, mu, +1) : step_offset_indexed(g, n, mu, +1);
     const int s_mu = (n.lex + f_mu) >> 1;
-#pragma unroll 1
+#pragma unroll(UNROLL ? 4 : 1)
     for (int nu = 0; nu < 4; nu++) {
         if (nu == mu) continue;
         int s_nup, s_num, s_diag;
