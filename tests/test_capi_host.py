@@ -39,6 +39,19 @@ def test_create_rejects_bad_descriptors():
         assert e.value.status in (g.GLAC_ERR_ARG, g.GLAC_ERR_CUDA)
         if e.value.status == g.GLAC_ERR_ARG:
             assert "even" in str(e.value)
+    # size limits are checked before any device call: V <= 2^29, 32-bit field
+    # offsets (FP64 V < 1.19e8, FP32 V < 2.68e8), Nt <= 1024
+    for dims, prec, words in [((512, 512, 512, 8), "fp32", "2^29"),
+                              ((256, 256, 256, 8), "fp64", "32-bit"),
+                              ((512, 256, 256, 8), "fp32", "32-bit"),
+                              ((4, 4, 4, 1026), "fp64", "Nt")]:
+        with pytest.raises(g.GlacError) as e:
+            g.Lattice(dims, precision=prec)
+        assert e.value.status == g.GLAC_ERR_ARG and words in str(e.value), str(e.value)
+    from glac_b200.ensemble import Ensemble
+    with pytest.raises(g.GlacError) as e:
+        Ensemble([(4, 4, 4, 8), (512, 256, 256, 8)], [6.0, 6.0], precision="fp32")
+    assert e.value.status == g.GLAC_ERR_ARG and "lattice 1" in str(e.value)
 
 
 def test_no_cpu_fallback_without_device():
