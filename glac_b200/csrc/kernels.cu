@@ -549,14 +549,14 @@ template <typename T> __device__ __forceinline__ AH8<T> ah_add(const AH8<T> &X, 
 // Clover of the (mu, nu) plane at n, projected: F = (C - C^+) - 1/3 i ImTr(C - C^+),
 // returned in the 8-real form; *plaq = ReTr(leaf1).  Links are re-read from
 // L1/L2 rather than held, to keep register pressure low.  C = leaf1 - leaf2 +
-// leaf3 - leaf4 as in the reference (mastersampler.cpp:175-207), summed in a
-// different order (pairs of leaves sharing their first link).  Not inlined: with
-// its own register allocation the calling kernels fit a 128-register cap
-// (4 blocks of 128 per SM) with a small spill, where the inlined form needs
-// ~180 registers (2 blocks); the autotuner picks between the two caps.
+// leaf3 - leaf4 as in the reference (mastersampler.cpp:175-207); FP32 sums the
+// leaves in a different order (pairs sharing their first link).  The FP64 form
+// runs as a non-inlined call (clover_ah_call): with its own register allocation
+// the calling kernels fit a 128-register cap with a small spill, where the
+// inlined FP64 form spills kilobytes; the autotuner picks among the caps.
 template <typename T>
-__device__ __noinline__ AH8<T> clover_ah(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu,
-                                            int nu, T &plaq) {
+__device__ __forceinline__ AH8<T> clover_ah_body(const LinkField<T> &L, const Geom &g, const Site &n, int p,
+                                                 int mu, int nu, T &plaq) {
     const int q = p ^ 1;
     const int s_n = n.lex >> 1;
     const int s_mup = lex_step(g, n, mu, +1) >> 1;           // n+mu      (q)
@@ -622,6 +622,20 @@ __device__ __noinline__ AH8<T> clover_ah(const LinkField<T> &L, const Geom &g, c
         F = proj_ah8(C);
     }
     return F;
+}
+
+template <typename T>
+__device__ __noinline__ AH8<T> clover_ah_call(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu,
+                                              int nu, T &plaq) {
+    return clover_ah_body<T>(L, g, n, p, mu, nu, plaq);
+}
+// FP32: inlined (the leaf-pair form fits the 128-register variant with a 4 B
+// spill); FP64: a call with its own register allocation.
+template <typename T>
+__device__ __forceinline__ AH8<T> clover_ah(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu,
+                                            int nu, T &plaq) {
+    if constexpr (sizeof(T) == 4) return clover_ah_body<T>(L, g, n, p, mu, nu, plaq);
+    else return clover_ah_call<T>(L, g, n, p, mu, nu, plaq);
 }
 
 // Re Tr(F G) for traceless anti-Hermitian F, G in the 8-real form:
