@@ -6,7 +6,7 @@ gauge-invariant features of a link's staple to the spread of that link's
 proposals; the staple is unchanged by the link's own update, so the proposal
 stays symmetric and the accept step of GLAC/system.cpp:333-361 keeps the chain
 exact.  The plain fixed-spread sampler is both its fallback (no network set)
-and its judge (plaquette, <Q^2>, tau_int).
+and the yardstick it is measured against (plaquette, <Q^2>, tau_int).
 
 Pipeline (all on the GPU through the C ABI; device buffers are torch tensors):
   collect_esj   plain-sampler sweeps; every `every` sweeps, expected-squared-jump
