@@ -180,8 +180,12 @@ extern "C" glac_status glac_measure_noalloc(const int dims[4], const double *dev
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    if (e != cudaSuccess) {
         g_err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+        return GLAC_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= 64) {
+        g_err = "device ordinal " + std::to_string(dev) + " beyond the 64 devices this entry point tracks";
         return GLAC_ERR_CUDA;
     }
     void *scratch = nullptr;
