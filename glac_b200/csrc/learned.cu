@@ -270,6 +270,9 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
             }
             // every thread takes the same branch, so no barrier below is skipped by some threads only
             ok = __syncthreads_and(wait_phase(bar, phase)) != 0;
+            // on a timeout the MMA may still be in flight: one more bounded wait
+            // before the loop ends and the TMEM is freed below
+            if (!ok) wait_phase(bar, phase);
             phase ^= 1u;
             fence_after();
             if (!ok) break;
