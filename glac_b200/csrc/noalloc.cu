@@ -20,6 +20,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 #include <string>
 
@@ -160,10 +161,26 @@ extern "C" glac_status glac_measure_noalloc(const int dims[4], const double *dev
         g_err = "null argument";
         return GLAC_ERR_ARG;
     }
+    // the kernel reads each link as nine 16-byte double2 words and writes
+    // doubles: a misaligned buffer is an argument error, not a device fault
+    if (reinterpret_cast<uintptr_t>(dev_links) % 16 != 0) {
+        g_err = "dev_links must be 16-byte aligned";
+        return GLAC_ERR_ARG;
+    }
+    if (reinterpret_cast<uintptr_t>(dev_obs) % 8 != 0) {
+        g_err = "dev_obs must be 8-byte aligned";
+        return GLAC_ERR_ARG;
+    }
+    // V = Nx Ny Nz Nt <= 2^31, checked before each product so it cannot wrap
+    const long long kMaxV = 1ll << 31;
     long long V = 1;
     for (int d = 0; d < 4; d++) {
         if (dims[d] < 2) {
             g_err = "every lattice extent must be at least 2";
+            return GLAC_ERR_ARG;
+        }
+        if ((long long)dims[d] > kMaxV / V) {
+            g_err = "lattice too large (V > 2^31)";
             return GLAC_ERR_ARG;
         }
         V *= dims[d];
@@ -172,10 +189,6 @@ extern "C" glac_status glac_measure_noalloc(const int dims[4], const double *dev
     if (Nt > kMaxSlots) {
         g_err = "Nt = " + std::to_string(Nt) + " exceeds the scratch capacity of " + std::to_string(kMaxSlots) +
                 " time slices";
-        return GLAC_ERR_ARG;
-    }
-    if (V > (1ll << 31)) {
-        g_err = "lattice too large (V > 2^31)";
         return GLAC_ERR_ARG;
     }
     int dev = 0;
@@ -188,11 +201,21 @@ extern "C" glac_status glac_measure_noalloc(const int dims[4], const double *dev
         g_err = "device ordinal " + std::to_string(dev) + " beyond the 64 devices this entry point tracks";
         return GLAC_ERR_CUDA;
     }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) {
+        g_err = std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e);
+        return GLAC_ERR_CUDA;
+    }
     void *scratch = nullptr;
     {
-        // first call on a device: resolve the device address of the scratch array
+        // The array's device address belongs to the module loaded in the current
+        // context; after cudaDeviceReset (a new primary context) it can move.
+        // Outside stream capture it is resolved afresh on every call; during a
+        // capture the address of this device's last uncaptured call is used.
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratch_ptr[dev]) {
+        if (cap == cudaStreamCaptureStatusNone) {
             void *p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess) {
@@ -200,6 +223,9 @@ extern "C" glac_status glac_measure_noalloc(const int dims[4], const double *dev
                 return GLAC_ERR_CUDA;
             }
             g_scratch_ptr[dev] = p;
+        } else if (!g_scratch_ptr[dev]) {
+            g_err = "the first call on a device must come before any stream capture";
+            return GLAC_ERR_STATE;
         }
         scratch = g_scratch_ptr[dev];
     }
@@ -214,7 +240,6 @@ extern "C" glac_status glac_measure_noalloc(const int dims[4], const double *dev
     L.p = dev_links;
     for (int d = 0; d < 4; d++) L.N[d] = dims[d];
     L.V = V;
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     k_measure_noalloc<<<dim3(K, Nt), kBlock, 0, st>>>(L, reinterpret_cast<double *>(scratch));
     k_finalize_noalloc<<<1, 32, 0, st>>>(Nt, K, (double)V, reinterpret_cast<const double *>(scratch), dev_obs);
     e = cudaGetLastError();

@@ -181,14 +181,18 @@ glac_status glac_accept_fed(int precision, double beta, long n_links, int n_hits
  * allocation would synchronise the device, deployments whose device memory is
  * fixed at load time -- this entry point measures [plaq, topc, energy,
  * topct[Nt]] of a field without allocating anything: dev_links is a device
- * pointer to the field in the host layout above (FP64), dev_obs a device
- * pointer to 3 + Nt doubles, stream a cudaStream_t (NULL: default stream); the
- * call is asynchronous on that stream.  Its only working memory is a fixed
+ * pointer to the field in the host layout above (FP64, 16-byte aligned),
+ * dev_obs a device pointer to 3 + Nt doubles (8-byte aligned), stream a
+ * cudaStream_t (NULL: default stream); the call is asynchronous on that stream.
+ * A misaligned pointer, an extent below 2 or V above 2^31 gives GLAC_ERR_ARG.
+ * Its only working memory is a fixed
  * 96 KiB device array inside this library (4096 partial-sum slots), held by
  * every GPU that loads the library until the process exits; Nt above 4096 is
- * rejected with GLAC_ERR_ARG.  The first call on a device resolves that array's
- * address (cudaGetSymbolAddress), so make the first call on each device outside
- * any stream capture.  All calls share the array and every call overwrites the
+ * rejected with GLAC_ERR_ARG.  Every call outside stream capture resolves that
+ * array's address in the current context (cudaGetSymbolAddress); a call made
+ * while its stream is capturing reuses the address of the device's last
+ * uncaptured call, so make the first call on each device outside any stream
+ * capture (otherwise GLAC_ERR_STATE).  All calls share the array and every call overwrites the
  * slots it reads, so nothing needs clearing between calls -- but calls that
  * overlap on the GPU (different streams, or different host threads, at the same
  * time) race on it and must be serialised by the caller.  Errors:
@@ -246,6 +250,15 @@ glac_status glac_mlp_init(glac_mlp *mlp, uint64_t seed, double eps_min, double e
  * Both round at the same points; at this network size mode 0 is the faster
  * (36.7 vs 84.2 us per 2M rows on B200). */
 glac_status glac_mlp_set_forward_mode(glac_mlp *mlp, int mode);
+/* Test export for the failure path of mode 1.  wait_ns (1 ns .. 10 s, default
+ * 1 s) bounds each completion wait of the tcgen05 kernel by the GPU's global
+ * timer; issue_mma = 0 makes the kernel issue no MMA, so its first wait runs
+ * out with nothing in flight: glac_mlp_forward then returns GLAC_ERR_TIMEOUT
+ * and the next call (issue_mma = 1) works normally.  If a wait runs out while
+ * an issued MMA is still in flight and a second wait of the same length does
+ * not see it drain, the call returns GLAC_ERR_TIMEOUT and every later mode-1
+ * call on this trainer returns GLAC_ERR_STATE.  No reference counterpart. */
+glac_status glac_mlp_test_tc_wait(glac_mlp *mlp, unsigned long long wait_ns, int issue_mma);
 glac_status glac_mlp_forward(glac_mlp *mlp, const float *dev_features, long long n, double eps_min, double eps_max,
                              float *dev_eps);
 /* Loss L = -(1/n) sum_i J_i(eps_i), J_i linear between the n_eps grid points

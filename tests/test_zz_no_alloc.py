@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from conftest import rel_err
+from conftest import assert_obs_close
 
 pytestmark = pytest.mark.gpu
 
@@ -39,6 +39,7 @@ def test_measure_noalloc_matches_context_path(oracle):
         with g.Lattice(dims, precision="fp64") as lat:
             lat.set_links(links)
             want = lat.measure()
+        assert_obs_close(want, oracle.observables(dims, links), 1e-12, f"{dims} context path vs oracle")
         dev_links = torch.from_numpy(links.reshape(-1)).cuda()
         dev_obs = torch.zeros(3 + dims[3], dtype=torch.float64, device="cuda")
         for call in range(2):
@@ -48,7 +49,8 @@ def test_measure_noalloc_matches_context_path(oracle):
             torch.cuda.synchronize()
             got = dev_obs.cpu().numpy()
             assert np.all(np.isfinite(got)), (dims, call)
-            assert rel_err(got, want) < 1e-12, (dims, call)
+            assert_obs_close(got, want, 1e-12, f"{dims} call {call} vs glac_measure")
+            assert_obs_close(got, oracle.observables(dims, links), 1e-12, f"{dims} call {call} vs oracle")
 
 
 def test_measure_noalloc_rejects_oversize():
@@ -57,3 +59,27 @@ def test_measure_noalloc_rejects_oversize():
     st = L.glac_measure_noalloc((ctypes.c_int * 4)(4, 4, 4, 5000), dummy, dummy, None)
     assert st == 1
     assert "scratch capacity" in L.glac_noalloc_error().decode()
+
+
+def test_measure_noalloc_rejects_misaligned_buffers():
+    # the field is read as 16-byte words and the output written as doubles:
+    # buffers off those boundaries are refused on the host, before any launch
+    import torch
+
+    L = _lib()
+    dims = (4, 4, 4, 4)
+    buf = torch.zeros(4 * 256 * 18 + 2, dtype=torch.float64, device="cuda")
+    obs = torch.zeros(3 + 4 + 1, dtype=torch.float64, device="cuda")
+    assert buf.data_ptr() % 16 == 0
+    st = L.glac_measure_noalloc((ctypes.c_int * 4)(*dims), buf.data_ptr() + 8, obs.data_ptr(), None)
+    assert st == 1 and "16-byte" in L.glac_noalloc_error().decode()
+    st = L.glac_measure_noalloc((ctypes.c_int * 4)(*dims), buf.data_ptr(), obs.data_ptr() + 4, None)
+    assert st == 1 and "8-byte" in L.glac_noalloc_error().decode()
+
+
+def test_measure_noalloc_rejects_volume_overflow():
+    # extents whose product wraps a 64-bit integer are refused before it is formed
+    L = _lib()
+    dummy = ctypes.c_void_p(256)
+    st = L.glac_measure_noalloc((ctypes.c_int * 4)(1 << 21, 1 << 21, 1 << 21, 2), dummy, dummy, None)
+    assert st == 1 and "too large" in L.glac_noalloc_error().decode()
