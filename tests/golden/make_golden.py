@@ -1,7 +1,8 @@
 """Generates the committed golden fixtures in this folder.
 
-Run in a container that holds the reference tree (its path is the REF_SRC
-default of oracle/Makefile).  Two kinds of fixture:
+Run where the reference tree exists: its GLAC folder is $GLAC_REF_SRC, by
+default ../reference/GLAC beside the repository (the default of
+oracle/Makefile too).  Three kinds of fixture:
 
 * ``testcore_fixtures.json`` -- the known-answer matrices of the reference's
   unit tests (GLAC/tests/unit_tests/testcore.cpp:31-232), read as text from
@@ -11,6 +12,14 @@ default of oracle/Makefile).  Two kinds of fixture:
   flow force (first 64 sites), exponentials, three RK3 flow steps, the
   MasterSamplerTopcXYZ observables before and after, and the first 64 links
   of one recorded Metropolis sweep (proposals, uniforms, decisions).
+* ``ref_4x4x4x8_b6_flow.npz`` -- a thermalised 4^3 x 8 field from the
+  reference's own Metropolis chain (System::update, beta = 6.0, 300 sweeps from
+  a seeded Haar field), the reference's MasterSamplerTopcXYZ observables before
+  and after each of 100 RK3 flow steps at eps = 0.01 (plaquette 0.589 -> 0.993,
+  |Q| >= 0.21 throughout, so every observable has a scale of its own), and the
+  first 64 links per direction of the field after the 100 steps.
+
+  python tests/golden/make_golden.py [testcore|ref4|flow]...   (default: all)
 """
 import json
 import os
@@ -22,7 +31,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-REF = "/root/reference/GLAC/tests/unit_tests/testcore.cpp"
+REF_SRC = os.environ.get("GLAC_REF_SRC", os.path.join(ROOT, "..", "reference", "GLAC"))
+REF = os.path.join(REF_SRC, "tests", "unit_tests", "testcore.cpp")
 
 
 def parse_testcore(path):
@@ -42,11 +52,13 @@ def parse_testcore(path):
     return out
 
 
-def main():
+def make_testcore():
     fx = parse_testcore(REF)
     with open(os.path.join(HERE, "testcore_fixtures.json"), "w") as f:
         json.dump(fx, f, indent=1, sort_keys=True)
 
+
+def make_ref4():
     from oracle.oracle import Oracle, Reference
     o, r = Oracle(), Reference()
     N = (4, 4, 4, 4)
@@ -76,5 +88,30 @@ def main():
     )
 
 
+def make_flow(nsteps=100, K=64):
+    from oracle.oracle import Oracle, Reference
+    o, r = Oracle(), Reference()
+    N = (4, 4, 4, 8)
+    r.configure(4, 8, beta=6.0, su3eps=0.24, flow_eps=0.01, nupdates=10, nflows=nsteps,
+                metropolis_seed=31.0, matrix_seed=37.0)
+    start, plaq, acc = r.metropolis_chain(o.haar_field(N, 101), 300)
+    cur = start
+    rows = [r.observables(cur)]
+    for _ in range(nsteps):
+        cur = r.flow(cur, 1)
+        rows.append(r.observables(cur))
+    np.savez_compressed(
+        os.path.join(HERE, "ref_4x4x4x8_b6_flow.npz"),
+        links=start, flow_eps=np.array([0.01]), observables=np.array(rows), links_end=cur[:, :K],
+        chain_plaquette=plaq, chain_acceptance=np.array([acc]),
+    )
+
+
+def main(which):
+    makers = {"testcore": make_testcore, "ref4": make_ref4, "flow": make_flow}
+    for name in which or list(makers):
+        makers[name]()
+
+
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])
