@@ -54,6 +54,8 @@ NCU_TRAFFIC_STAGE0_FP32 = 636109568 + 837838592  # bytes, one ncu capture of the
 # (sm__sass_thread_inst_executed_op_{ffma,fadd,fmul}_pred_on) on the 32^3x64 launch
 FLOPS_PER_SITE_STAGE0_FP32 = 4 * (2 * 1547 + 59 + 95)
 SM_COUNT, FP32_LANES_PER_SM = 148, 128
+# Metropolis: algorithmic bytes per link update in FP32 (9 link transfers x 72 B)
+METRO_BYTES_FP32 = 9 * 72
 
 
 def load_peaks():
@@ -119,27 +121,78 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference (oracle/_ref) or the oracle port, one process per core
+# CPU baseline and reference arm: the reference's own flow + measurement
+# (oracle/_ref, the GLAC sources compiled with the reference's -O3 -march=native
+# where the host CPU allows, else the oracle C port), one process per core on
+# independent 32^3 x 64 lattices -- the reference parallelises only through MPI
+# domain decomposition, which this single-node build does not have.
 # ---------------------------------------------------------------------------
-def _cpu_worker(args):
-    kind, dims, nsteps, seed = args
+# peak resident memory of one reference process flowing and measuring a lattice,
+# per site (measured: 9.53 GB peak at 32^3 x 64 = 4545 B per site, rounded up)
+REF_BYTES_PER_SITE = 5000
+
+
+def host_memory_available():
+    """Bytes this process may still use: MemAvailable, capped by a cgroup limit."""
+    avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    for lim, use in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                     ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        try:
+            with open(lim) as f:
+                raw = f.read().strip()
+            if raw == "max":
+                continue
+            with open(use) as f:
+                room = int(raw) - int(f.read().strip())
+            avail = room if avail is None else min(avail, room)
+        except (OSError, ValueError):
+            continue
+    return avail
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown CPU"
+
+
+def _cpu_worker(args, barrier, results):
+    """One process: warm up on an 8^3 x 16 lattice, build its own Haar field at
+    dims, wait for the others, then time nsteps x (RK3 step + measurement)."""
+    idx, kind, dims, nsteps, seed, warm = args
     sys.path.insert(0, ROOT)
     from oracle.oracle import Oracle, Reference
     o = Oracle()
+    r = Reference() if kind == "reference" else None
+    if warm and r is not None:
+        r.configure(8, 16, beta=BETA, flow_eps=FLOW_EPS, nflows=warm)
+        r.time_flow_measure(o.haar_field((8, 8, 8, 16), seed), warm)
     links = o.haar_field(dims, seed)
-    if kind == "reference":
-        r = Reference()
+    if r is not None:
         r.configure(dims[0], dims[3], beta=BETA, flow_eps=FLOW_EPS, nflows=nsteps)
-        t0 = time.perf_counter()
+    barrier.wait(timeout=900)
+    if r is not None:
         dt = r.time_flow_measure(links, nsteps)
-        return dt, time.perf_counter() - t0
-    t0 = time.perf_counter()
-    cur = links
-    for _ in range(nsteps):
-        cur = o.flow(dims, cur, FLOW_EPS, 1)
-        o.observables(dims, cur)
-    dt = time.perf_counter() - t0
-    return dt, dt
+    else:
+        t0 = time.perf_counter()
+        cur = links
+        for _ in range(nsteps):
+            cur = o.flow(dims, cur, FLOW_EPS, 1)
+            o.observables(dims, cur)
+        dt = time.perf_counter() - t0
+    results.put((idx, dt))
 
 
 def cpu_kind():
@@ -147,22 +200,49 @@ def cpu_kind():
     return "reference" if os.path.exists(REF_SO) else "port"
 
 
-def cpu_flow_rate(nsteps_per_worker: int, dims=(8, 8, 8, 16), workers=None):
-    """Aggregate CPU site-steps/s of flow + per-step observables over all host cores."""
+def cpu_flow_rate(nsteps_per_proc: int = 1, dims=DIMS, procs=None, warm=0):
+    """Aggregate site-steps/s of the reference's flow + per-step observables on
+    this host: `procs` processes (default: one per core, as many as host memory
+    holds) each flow and measure their own lattice for nsteps_per_proc steps,
+    started together; value = all lattice-steps / the slowest process's time."""
     kind = cpu_kind()
-    workers = workers or os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
     V = int(np.prod(dims))
-    with ctx.Pool(workers) as pool:
-        t0 = time.perf_counter()
-        res = pool.map(_cpu_worker, [(kind, dims, nsteps_per_worker, 1000 + i) for i in range(workers)])
-        wall = time.perf_counter() - t0
-    slowest = max(r[0] for r in res)
-    value = workers * V * nsteps_per_worker / slowest
-    sample = (f"{workers} processes x {nsteps_per_worker} steps (RK3 flow + MasterSamplerTopcXYZ) on independent "
-              f"{dims[0]}^3x{dims[3]} Haar fields; {'GLAC sources compiled as oracle/_ref' if kind == 'reference' else 'oracle C port'}")
-    return {"value": value, "unit": UNIT, "cores": workers, "kind": kind, "sample": sample,
-            "wall_s": round(wall, 2), "per_core": value / workers}
+    cores = os.cpu_count() or 1
+    avail = host_memory_available()
+    by_mem = max(1, int(0.8 * avail // (REF_BYTES_PER_SITE * V))) if avail else cores
+    procs = procs or max(1, min(cores, by_mem))
+    build = "oracle C port (reference library absent)"
+    if kind == "reference":
+        from oracle.oracle import ref_library
+        build = f"GLAC sources compiled as oracle/_ref ({ref_library()[1]})"
+    ctx = mp.get_context("spawn")
+    barrier, results = ctx.Barrier(procs), ctx.Queue()
+    workers = [ctx.Process(target=_cpu_worker, args=((i, kind, dims, nsteps_per_proc, 1000 + i, warm), barrier,
+                                                     results)) for i in range(procs)]
+    t0 = time.perf_counter()
+    for w in workers:
+        w.start()
+    res = [results.get(timeout=3600) for _ in workers]
+    for w in workers:
+        w.join()
+    wall = time.perf_counter() - t0
+    if any(w.exitcode != 0 for w in workers):
+        raise RuntimeError("a CPU baseline process failed")
+    slowest = max(dt for _, dt in res)
+    value = procs * nsteps_per_proc * V / slowest
+    sample = (f"{procs} processes x {nsteps_per_proc} step(s) (RK3 flow + MasterSamplerTopcXYZ, eps={FLOW_EPS}) "
+              f"on independent {dims[0]}^3x{dims[3]} Haar fields, started together; {build}; "
+              f"{cores} cores ({cpu_model()}), process count limited by "
+              f"{'host memory' if procs < cores else 'cores'} at {REF_BYTES_PER_SITE * V / 1e9:.1f} GB each")
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample,
+            "wall_s": round(wall, 2), "timed_s": round(slowest, 2), "per_core": value / procs,
+            "lattice_steps": procs * nsteps_per_proc}
+
+
+def bench_config(world):
+    """The workload's config, printed identically by both arms."""
+    return {"workload": WORKLOAD, "dims": list(DIMS), "beta": BETA, "flow_eps": FLOW_EPS,
+            "l2": "field 604 MB FP32 > 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"}
 
 
 # ---------------------------------------------------------------------------
@@ -205,7 +285,7 @@ def run_gpu(args):
 
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu_base = cpu_flow_rate(args.cpu_steps)  # before the first GPU call (spawned pool)
+        cpu_base = cpu_flow_rate(args.cpu_steps)  # before the first GPU call (spawned processes)
 
     import glac_b200 as g
 
@@ -238,6 +318,11 @@ def run_gpu(args):
     start = np.empty((4, V, 18))
     L.get_links(start)
     metro_rate = world * 4 * V * 20 / t_metro
+    # Metropolis roofline: compulsory traffic of a (mu, parity) sub-sweep per
+    # updated link = the link read and written (2), the three other directions'
+    # links of both parities (6) and the other parity's mu links (1): 9 x 72 B
+    metro_roofline = {"achieved": round(METRO_BYTES_FP32 * metro_rate / world / 1e9, 1), "unit": "GB/s",
+                      "algorithmic_bytes_per_link_update": METRO_BYTES_FP32}
 
     obs_buf = np.empty((args.steps + 1, 3 + DIMS[3]))
 
@@ -258,7 +343,10 @@ def run_gpu(args):
     # roofline of the flow-stage kernel: CUDA events around each stage launch on
     # the lattice's stream, averaged over reps RK3 steps
     reps = max(3, min(args.steps, 20))
+    clk_st = ClockSampler(local)
+    clk_st.start()
     st = np.array(L.flow_stage_times(reps))
+    stage_clocks = clk_st.stop()
     hbm_peak, peak_kind = load_peaks()
     # dominant kernel: the stage-0 flow launch; algorithmic bytes = 4 links read
     # + 4 links written + force written per site (704 B FP32)
@@ -272,6 +360,8 @@ def run_gpu(args):
                 "kernel": "k_flow_stage<float, morningstar, stage 0>",
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind,
                 "stage_ms": [round(x * 1e3, 4) for x in st],
+                "stage_ms_how": (f"CUDA events around each stage launch over {reps} RK3 steps right after the timed "
+                                 f"region; SM clock median {stage_clocks.get('sm_mhz')} MHz meanwhile"),
                 "binding_unit": "FP32 FMA pipe (60 % busy per ncu; HBM 25 %)"}
     # the binding unit: FP32 FLOP/s of the same launch against the FP32 peak at the
     # median SM clock sampled during the timed region (148 SMs x 128 lanes x 2 FLOP per FMA)
@@ -361,17 +451,23 @@ def run_gpu(args):
             tune_e = E.autotune(2)
             E.run(100, 200)  # capture
             _, obs_e, sec_e = E.run(100, 200)
+            # the two phases as graphs of their own, for a rate in each unit
+            E.run(100, 0)
+            _, _, sec_sweeps = E.run(100, 0)
+            E.run(0, 200)
+            _, _, sec_flow = E.run(0, 200)
         sites_e = int(sum(np.prod(d) for d in dims_l))
-        ens_extra = {"lattices": 64, "sites": sites_e, "graph_gpu_s": sec_e,
-                     "link_updates_plus_flow_site_steps_per_s": sites_e * (4 * 100 + 200) / sec_e,
+        ens_extra = {"lattices": 64, "sites": sites_e, "schedule": "100 sweeps + 200 flow steps with observables",
+                     "graph_gpu_s": sec_e,
+                     "sweeps_graph_gpu_s": sec_sweeps, "link_updates_per_s": 4 * sites_e * 100 / sec_sweeps,
+                     "flow_graph_gpu_s": sec_flow, "flow_site_steps_per_s": sites_e * 200 / sec_flow,
                      "autotune_chosen": tune_e["chosen"], "plaq_after_flow_mean": float(np.mean([o[-1, 0] for o in obs_e]))}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_main / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Haar + 600 Metropolis sweeps)",
-        "config": {"workload": WORKLOAD, "dims": list(DIMS), "beta": BETA, "flow_eps": FLOW_EPS,
-                   "l2": "field 604 MB FP32 > 126 MB L2 (no flush needed)", "parallelism": f"replicas x{world}"},
+        "config": bench_config(world),
         "roofline": roofline,
         "cpu_baseline": cpu_base,
         "e2e": e2e,
@@ -381,6 +477,8 @@ def run_gpu(args):
             "flow_site_steps_per_s_no_obs": rate_noobs,
             "flow_site_steps_per_s_fp64_with_obs": rate64,
             "metropolis_link_updates_per_s_fp32": metro_rate,
+            "metropolis_roofline_fp32": dict(metro_roofline, peak=hbm_peak,
+                                             frac=round(metro_roofline["achieved"] / hbm_peak, 4)),
             "metropolis_link_updates_per_s_fp64": metro64_rate,
             "learned": learned_extra,
             "ensemble_64_uneven": ens_extra,
@@ -400,32 +498,30 @@ def run_gpu(args):
 
 
 def run_reference(args):
+    """The reference's own CPU path on this host's cores at the benchmark's
+    lattice (32^3 x 64): one process per core (as many as host memory holds),
+    each flowing and measuring its own lattice; every process runs
+    max(1, steps // processes) steps, so the run stays within minutes (one
+    32^3 x 64 step of the reference takes minutes on one core).  Warm-up: W
+    steps of an 8^3 x 16 lattice in every process, untimed."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
-    workers = os.cpu_count() or 1
-    kind = cpu_kind()
-    dims = (8, 8, 8, 16)
-    V = int(np.prod(dims))
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(workers) as pool:
-        if args.warmup > 0:
-            pool.map(_cpu_worker, [(kind, dims, 1, 50 + i) for i in range(workers)])
-        t0 = time.perf_counter()
-        res = pool.map(_cpu_worker, [(kind, dims, args.steps, 1000 + i) for i in range(workers)])
-        wall = time.perf_counter() - t0
-    slowest = max(r[0] for r in res)
-    value = workers * V * args.steps / slowest
-    sample = (f"per step: each of {workers} processes runs 1 RK3 flow step + MasterSamplerTopcXYZ on its own "
-              f"{dims[0]}^3x{dims[3]} lattice ({'GLAC sources compiled as oracle/_ref' if kind == 'reference' else 'oracle C port'})")
+    cores = os.cpu_count() or 1
+    V = int(np.prod(DIMS))
+    avail = host_memory_available()
+    procs = max(1, min(cores, int(0.8 * avail // (REF_BYTES_PER_SITE * V)) if avail else cores))
+    per_proc = max(1, args.steps // procs)
+    base = cpu_flow_rate(per_proc, DIMS, procs, warm=args.warmup)
+    value = base["value"]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": slowest / args.steps * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": V / value * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded Haar)",
-            "config": {"workload": WORKLOAD, "dims": list(DIMS), "beta": BETA, "flow_eps": FLOW_EPS},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": kind, "sample": sample},
+            "data": "synthetic (seeded Haar)", "config": bench_config(world),
+            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "wall_s": round(wall, 2)}
+            "lattice_steps_timed": base["lattice_steps"], "timed_s": base["timed_s"], "wall_s": base["wall_s"],
+            "ms_per_step_note": "aggregate: 1e3 x sites / value (time per lattice-step of the whole host)"}
     print(json.dumps(line))
 
 
@@ -515,7 +611,7 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-steps", type=int, default=25)
+    ap.add_argument("--cpu-steps", type=int, default=1, help="32^3x64 steps per process of the CPU baseline")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-lattice ensemble leg")

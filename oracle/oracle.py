@@ -7,8 +7,12 @@ imports this module.
 * :class:`Oracle` -- the project's C restatement (``oracle/liboracle.so``,
   source ``oracle/glac_oracle.c``), always available once built.
 * :class:`Reference` -- the reference GLAC sources compiled into
-  ``oracle/_ref/libglacref.so`` (recipe ``oracle/Makefile``).  Built only where
-  the reference tree exists; the prebuilt library travels with the repository
+  ``oracle/_ref/libglacref.so`` (portable, -march=x86-64-v3) and
+  ``oracle/_ref/native/libglacref.so`` (the reference's own -O3 -march=native,
+  for the CPU that built it; used only on a host whose ISA flags include that
+  CPU's, see :func:`ref_library`).  Recipe ``oracle/Makefile``.  Built only
+  where the reference tree exists ($GLAC_REF_SRC, default ../reference/GLAC
+  beside the repository); the prebuilt libraries travel with the repository
   copy to other machines.
 
 Field layout for every call: float64 array of shape (4, V, 18), sites in
@@ -25,7 +29,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libglacref.so")
-REF_SRC = "/root/reference/GLAC"
+REF_NATIVE_SO = os.path.join(HERE, "_ref", "native", "libglacref.so")
+REF_NATIVE_FLAGS = os.path.join(HERE, "_ref", "native", "cpu_flags.txt")
+REF_SRC = os.environ.get("GLAC_REF_SRC", os.path.normpath(os.path.join(HERE, "..", "..", "reference", "GLAC")))
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
@@ -34,11 +40,49 @@ _u32 = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 
 
 def build(ref: bool = True) -> None:
-    """Compile the C restatement, and the reference library when its sources exist."""
+    """Compile the C restatement, and the reference libraries when its sources exist."""
     targets = ["oracle"]
     if ref and os.path.isdir(REF_SRC):
-        targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
+        targets += ["ref", "ref-native"]
+    subprocess.run(["make", "-s", "-C", HERE, "-j8", f"REF_SRC={REF_SRC}", *targets], check=True)
+
+
+def _cpu_flags(path="/proc/cpuinfo"):
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def ref_library():
+    """(path, build) of the reference library to load on this host.
+
+    The -march=native build when it exists and this CPU has every ISA flag of
+    the CPU that compiled it (so it cannot hit an unsupported instruction),
+    else the portable -march=x86-64-v3 build.
+    """
+    if os.path.exists(REF_NATIVE_SO) and os.path.exists(REF_NATIVE_FLAGS):
+        with open(REF_NATIVE_FLAGS) as f:
+            need = _isa_flags(f.read().split())
+        if need and need <= _isa_flags(_cpu_flags()):
+            return REF_NATIVE_SO, "-O3 -march=native"
+    return REF_SO, "-O3 -march=x86-64-v3"
+
+
+# /proc/cpuinfo flags that name instruction-set extensions a compiler may emit
+# (the rest -- hypervisor, clock and power features -- differ between hosts
+# with the same instruction set)
+_ISA_PREFIXES = ("sse", "ssse", "avx", "fma", "f16c", "bmi", "amx", "movbe", "popcnt", "abm", "adx", "sha",
+                 "vaes", "vpclmul", "gfni", "aes", "pclmul", "cx16", "lzcnt", "rdrand", "rdseed", "clflushopt",
+                 "clwb", "xsave", "movdir", "serialize", "prefetchw", "3dnowprefetch")
+
+
+def _isa_flags(flags):
+    return {f for f in flags if f.startswith(_ISA_PREFIXES)}
 
 
 def _dims(N):
@@ -198,12 +242,16 @@ class Oracle:
 class Reference:
     """The reference's own classes, compiled from its sources (see oracle/Makefile)."""
 
-    def __init__(self, path: str = REF_SO):
-        if not os.path.exists(path):
-            if os.path.isdir(REF_SRC):
+    def __init__(self, path: str | None = None):
+        if path is None:
+            if not os.path.exists(REF_SO) and os.path.isdir(REF_SRC):
                 build(ref=True)
-            else:
-                raise FileNotFoundError(f"{path} is not built and the reference sources are absent")
+            path, self.build_flags = ref_library()
+        else:
+            self.build_flags = "given path"
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built and the reference sources are absent")
+        self.path = path
         lib = C.CDLL(path)
         lib.ref_configure.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_char_p,
                                       C.c_double, C.c_double, C.c_int, C.c_int]
