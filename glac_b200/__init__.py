@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
     L.glac_mlp_init.argtypes = [P, C.c_uint64, C.c_double, C.c_double, C.c_double]
     L.glac_mlp_forward.argtypes = [P, C.c_void_p, C.c_longlong, C.c_double, C.c_double, C.c_void_p]
     L.glac_mlp_set_forward_mode.argtypes = [P, C.c_int]
+    L.glac_mlp_test_tc_wait.argtypes = [P, C.c_ulonglong, C.c_int]
     L.glac_mlp_loss_grad.argtypes = [P, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, _dp,
                                      C.POINTER(C.c_double), C.c_void_p]
     L.glac_mlp_train.argtypes = [P, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, _dp, C.c_int, C.c_longlong,

@@ -122,7 +122,6 @@ constexpr int kBar = 24576;    // mbarrier
 constexpr int kSlot = 24584;   // TMEM base address written by tcgen05.alloc
 constexpr int kSmem = 61440;   // requested, so that at most 3 CTAs (3 x 128 TMEM columns) share an SM
 constexpr int kCols = 128;     // TMEM columns: D1 0-31, D2 32-63, D3 64-79
-constexpr uint32_t kWaitLimit = 1u << 22;
 
 // byte offset of BF16 element (row, k) in a K-major, no-swizzle operand of `rows` rows
 __device__ __forceinline__ uint32_t kmaj(int row, int k, int rows) {
@@ -147,18 +146,26 @@ __device__ __forceinline__ void commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
 }
-// bounded wait for the mbarrier phase; false on timeout
-__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t phase) {
-    for (uint32_t it = 0; it < kWaitLimit; it++) {
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Wait for the mbarrier phase for at most limit_ns nanoseconds of the global
+// timer (each try_wait suspends for at most kSuspendNs); false on timeout.
+constexpr uint32_t kSuspendNs = 1000;
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t phase, uint64_t limit_ns) {
+    const uint64_t t0 = globaltimer_ns();
+    for (;;) {
         uint32_t done;
-        asm volatile("{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        asm volatile("{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2, %3;\n\t"
                      "selp.b32 %0, 1, 0, P;\n\t}\n"
                      : "=r"(done)
-                     : "r"(bar), "r"(phase)
+                     : "r"(bar), "r"(phase), "r"(kSuspendNs)
                      : "memory");
         if (done) return true;
+        if (globaltimer_ns() - t0 > limit_ns) return false;
     }
-    return false;
 }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -180,9 +187,17 @@ __device__ __forceinline__ void ld32(uint32_t taddr, float v[32]) {
 }
 }  // namespace tcf
 
+// err (atomicMax): 1 = a completion wait ran out and the tensor-core pipeline
+// was drained before the TMEM was freed; 2 = it was still not drained after a
+// second wait of the same length (the TMEM is freed all the same, as a CTA must
+// before it exits, so the caller must stop using this library's tensor-core
+// path).  issue = 0 is a test mode: no MMA and no commit are issued, so the
+// first wait runs out with nothing in flight (the timeout path, without a
+// fault or a hang).
 __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict__ P, const float *__restrict__ feat,
                                                         long long n, float eps_min, float eps_max,
-                                                        float *__restrict__ eps_out, int *__restrict__ err) {
+                                                        float *__restrict__ eps_out, int *__restrict__ err,
+                                                        unsigned long long wait_ns, int issue) {
     using namespace tcf;
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -224,7 +239,7 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
     const uint32_t tmem = *slot;
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     uint32_t phase = 0;
-    bool ok = true;
+    bool ok = true, drained = true;
     const long long tiles = (n + 127) / 128;
     // this thread's feature row of a tile (zeros past the end)
     auto fetch = [&](long long tile, float4 &a, float4 &b) {
@@ -262,17 +277,17 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
             const int B = layer == 0 ? kB1 : (layer == 1 ? kB2 : kB3);
             const int brows = layer == 2 ? 16 : 32, N = layer == 2 ? 16 : 32, ksteps = layer == 0 ? 1 : 2;
             const uint32_t dcol = 32u * (uint32_t)layer;
-            if (tid == 0) {
+            if (tid == 0 && issue) {
                 for (int ks = 0; ks < ksteps; ks++)
                     mma(tmem + dcol, sdesc(sbase + A + ks * 2 * 128 * 16, 128),
                         sdesc(sbase + B + ks * 2 * brows * 16, brows), idesc(N), ks > 0 ? 1u : 0u);
                 commit(bar);
             }
             // every thread takes the same branch, so no barrier below is skipped by some threads only
-            ok = __syncthreads_and(wait_phase(bar, phase)) != 0;
-            // on a timeout the MMA may still be in flight: one more bounded wait
-            // before the loop ends and the TMEM is freed below
-            if (!ok) wait_phase(bar, phase);
+            ok = __syncthreads_and(wait_phase(bar, phase, wait_ns)) != 0;
+            // on a timeout an issued MMA may still be in flight: one more bounded
+            // wait before the loop ends and the TMEM is freed below
+            if (!ok && issue) drained = __syncthreads_and(wait_phase(bar, phase, wait_ns)) != 0;
             phase ^= 1u;
             fence_after();
             if (!ok) break;
@@ -297,7 +312,7 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
             }
         }
     }
-    if (!ok && err) atomicExch(err, 1);
+    if (!ok && err && tid == 0) atomicMax(err, drained ? 1 : 2);
     fence_before();
     __syncthreads();
     fence_after();
@@ -306,12 +321,13 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
 }
 
 void launch_mlp_forward_tc(const float *params, const float *features, long long n, float eps_min, float eps_max,
-                           float *eps_out, int *err, cudaStream_t st) {
+                           float *eps_out, int *err, unsigned long long wait_ns, int issue, cudaStream_t st) {
     // per device (cheap): the attribute is not shared between devices
     cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf::kSmem);
     const long long tiles = (n + 127) / 128;
     const int grid = (int)(tiles < 3 * 148 ? tiles : 3 * 148);
-    k_mlp_forward_tc<<<grid, 128, tcf::kSmem, st>>>(params, features, n, eps_min, eps_max, eps_out, err);
+    k_mlp_forward_tc<<<grid, 128, tcf::kSmem, st>>>(params, features, n, eps_min, eps_max, eps_out, err, wait_ns,
+                                                    issue);
 }
 
 // ---------------------------------------------------------------------------
@@ -582,6 +598,9 @@ struct glac_mlp {
     uint32_t *pack = nullptr;
     int *err_dev = nullptr;  // wait-timeout flag of the tcgen05 kernel
     int forward_mode = 0;    // 0: the sampler's warp-level routine, 1: tcgen05 tiles
+    unsigned long long tc_wait_ns = 1000000000ull;  // completion-wait limit of the tcgen05 kernel (1 s)
+    int tc_issue = 1;        // 0: test mode, the tcgen05 kernel issues no MMA (its waits run out)
+    bool tc_broken = false;  // a tcgen05 pass timed out without draining: tensor-core path refused
     int step = 0;
     std::string err;
 };
@@ -744,14 +763,23 @@ glac_status glac_mlp_forward(glac_mlp *M, const float *dev_features, long long n
             mck(cudaStreamSynchronize(M->stream), "sync");
             return GLAC_OK;
         }
+        if (M->tc_broken) {
+            M->err = "an earlier tensor-core pass did not drain after its wait limit; mode 1 is disabled";
+            return GLAC_ERR_STATE;
+        }
         if (!M->err_dev) mck(cudaMalloc(&M->err_dev, sizeof(int)), "alloc");
         mck(cudaMemsetAsync(M->err_dev, 0, sizeof(int), M->stream), "memset");
         launch_mlp_forward_tc(M->params, dev_features, n, (float)eps_min, (float)eps_max, dev_eps, M->err_dev,
-                              M->stream);
+                              M->tc_wait_ns, M->tc_issue, M->stream);
         mck(cudaGetLastError(), "forward (tcgen05)");
         int flag = 0;
         mck(cudaMemcpyAsync(&flag, M->err_dev, sizeof(int), cudaMemcpyDeviceToHost, M->stream), "D2H");
         mck(cudaStreamSynchronize(M->stream), "sync");
+        if (flag == 2) {
+            M->tc_broken = true;
+            M->err = "tensor-core pass did not complete within its wait limit, nor drain after a second wait";
+            return GLAC_ERR_TIMEOUT;
+        }
         if (flag) {
             M->err = "tensor-core pass did not complete within its wait limit";
             return GLAC_ERR_TIMEOUT;
@@ -763,6 +791,13 @@ glac_status glac_mlp_forward(glac_mlp *M, const float *dev_features, long long n
 glac_status glac_mlp_set_forward_mode(glac_mlp *M, int mode) {
     if (!M || (mode != 0 && mode != 1)) return GLAC_ERR_ARG;
     M->forward_mode = mode;
+    return GLAC_OK;
+}
+
+glac_status glac_mlp_test_tc_wait(glac_mlp *M, unsigned long long wait_ns, int issue_mma) {
+    if (!M || wait_ns == 0 || wait_ns > 10000000000ull || (issue_mma != 0 && issue_mma != 1)) return GLAC_ERR_ARG;
+    M->tc_wait_ns = wait_ns;
+    M->tc_issue = issue_mma;
     return GLAC_OK;
 }
 

@@ -95,6 +95,11 @@ class ProposalNet:
         """0: the sampler's warp-level routine (default); 1: tcgen05 tensor-core tiles."""
         self._ck(lib().glac_mlp_set_forward_mode(self._h, int(mode)))
 
+    def set_tc_wait(self, wait_ns: int, issue_mma: bool = True):
+        """Test hook of mode 1: the completion-wait limit of the tcgen05 kernel in
+        ns, and (issue_mma=False) a pass that issues no MMA so that its wait runs out."""
+        self._ck(lib().glac_mlp_test_tc_wait(self._h, int(wait_ns), int(bool(issue_mma))))
+
     def forward(self, features, eps_min: float, eps_max: float):
         torch = _torch()
         f = features.contiguous()

@@ -130,6 +130,30 @@ def test_tensor_core_and_warp_inference_agree(g, torch, learned):
     assert np.median(d) < 1e-6 and d.max() < 5e-3
 
 
+def test_tensor_core_wait_timeout_is_reported_and_recovers(g, torch, learned):
+    # The tcgen05 kernel bounds every completion wait by the GPU's global timer.
+    # With no MMA issued (test mode) its first wait runs out with nothing in
+    # flight: the call returns GLAC_ERR_TIMEOUT, the device stays usable, and the
+    # next normal pass on the same trainer gives the right spreads.
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((1000, 8)).astype(np.float32)
+    P = random_params(5)
+    want = mlp.spread(P, X, f32(0.03)[()], f32(0.9)[()], emulate=True)
+    Xd = torch.from_numpy(X).cuda()
+    with learned.ProposalNet() as net:
+        net.params = P
+        net.set_forward_mode(1)
+        net.set_tc_wait(2_000_000, issue_mma=False)  # 2 ms
+        with pytest.raises(g.GlacError) as e:
+            net.forward(Xd, 0.03, 0.9)
+        assert e.value.status == g.GLAC_ERR_TIMEOUT
+        net.set_tc_wait(1_000_000_000, issue_mma=True)
+        got = net.forward(Xd, 0.03, 0.9).cpu().numpy()
+    d = np.abs(got - want)
+    assert np.median(d) < 1e-5 and d.max() < 5e-3
+    torch.cuda.synchronize()
+
+
 def test_gradient_matches_oracle(g, torch, learned):
     rng = np.random.default_rng(3)
     n, K = 5000, 16
