@@ -180,6 +180,164 @@ template void launch_flow_stage<float>(const Geom &, const LinkField<float> &, c
                                        const ForceField<float> &, int, int, double, double, int, cudaStream_t);
 
 // ---------------------------------------------------------------------------
+// Flow stage 0 fused with the measurement of its input field.
+//
+// The clover of the (mu, nu) plane at n is the sum of its four counterclockwise
+// leaves, and the staple pieces that stage 0 computes for the link U_mu(n) are
+// three of each leaf's four links:
+//   S_up  = U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+,  S_low = U_nu(n+mu-nu)^+ U_mu(n-nu)^+ U_nu(n-nu),
+//   leaf1(n) = U S_up,  leaf4(n) = (U S_low)^+,  leaf2(n+mu) = S_up U,  leaf3(n+mu) = (S_low U)^+
+// with U = U_mu(n).  With P(X) = (X - X^+) - 1/3 Tr(X - X^+) (linear, P(X^+) = -P(X)),
+// the projected clover F_munu(n) = P(leaf1 + leaf2 + leaf3 + leaf4)(n) is
+//   F_munu(n) = P(U W)(n) + P(W U)(n - mu),   W = S_up - S_low,
+// two products per plane once the staple is known, against ten in the
+// stand-alone observables kernel (GLAC/observables/mastersamplertopcxyz.cpp:
+// 253-340 builds each leaf from four links).  Each of the six planes is taken
+// by one link direction (mu = 0: nu = 1, 2; mu = 1: nu = 2, 3; mu = 2: nu = 3;
+// mu = 3: nu = 0, stored as -F_30 = F_03); the thread writes P(U W) into the
+// plane's "local" slot at n and P(W U) into its "forward" slot at n + mu, and
+// ReTr(U S_up) (the plaquette of the plane at n) into its direction's
+// plaquette slot.  k_obs_combine then adds the two slots of each plane per
+// site and reduces plaquette, Q(t) and E exactly as the observables kernel.
+// ---------------------------------------------------------------------------
+// (C - C^+) made traceless, in the 8-real form: diagonal 2 i Im C_ii minus a
+// third of its trace, off-diagonal C_ij - conj(C_ji).  Linear in C.
+template <typename T> __device__ __forceinline__ AH8<T> proj_ah8(const M3<T> &C) {
+    AH8<T> F;
+    const T two = T(2);
+    const T tr = (C(0, 0).im + C(1, 1).im + C(2, 2).im) * T(2.0 / 3.0);
+    F.a = two * C(0, 0).im - tr;
+    F.d = two * C(1, 1).im - tr;
+    F.b = cx(C(0, 1).re - C(1, 0).re, C(0, 1).im + C(1, 0).im);
+    F.c = cx(C(0, 2).re - C(2, 0).re, C(0, 2).im + C(2, 0).im);
+    F.e = cx(C(1, 2).re - C(2, 1).re, C(1, 2).im + C(2, 1).im);
+    return F;
+}
+template <typename T> __device__ __forceinline__ AH8<T> ah_add(const AH8<T> &X, const AH8<T> &Y) {
+    AH8<T> Z;
+    Z.a = X.a + Y.a;
+    Z.d = X.d + Y.d;
+    Z.b = X.b + Y.b;
+    Z.c = X.c + Y.c;
+    Z.e = X.e + Y.e;
+    return Z;
+}
+
+// plane index of (a, b), a < b: 01 0, 02 1, 03 2, 12 3, 13 4, 23 5
+__host__ __device__ constexpr int plane_of(int a, int b) { return a == 0 ? b - 1 : (a == 1 ? b + 1 : 5); }
+// the planes link direction mu takes (nu, or -1)
+__device__ __forceinline__ bool meas_takes(int mu, int nu) {
+    return (mu == 0 && (nu == 1 || nu == 2)) || (mu == 1 && (nu == 2 || nu == 3)) || (mu == 2 && nu == 3) ||
+           (mu == 3 && nu == 0);
+}
+
+template <typename T> __device__ __forceinline__ AH8<T> ah_neg_if(const AH8<T> &F, bool neg) {
+    return neg ? ah_scale(T(-1), F) : F;
+}
+
+template <typename T, int KIND>
+__device__ __forceinline__ void flow_stage0_meas_body(const Geom &g, const LinkField<T> &in, const LinkField<T> &out,
+                                                      const ForceField<T> &zf, const CloverParts<T> &cp, T alpha,
+                                                      int bx) {
+    const int plane = bx & 7;
+    const int s = (bx >> 3) * 128 + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int mu = plane >> 1, p = plane & 1, q = p ^ 1;
+    const Site n = site_from_ps(g, p, s);
+    const int f_mu = sizeof(T) == 4 ? step_offset(g, n, mu, +1) : step_offset_indexed(g, n, mu, +1);
+    const int s_mu = (n.lex + f_mu) >> 1;
+    M3<T> A;
+    set_zero(A);
+    T plaq = T(0);
+#pragma unroll 1
+    for (int nu = 0; nu < 4; nu++) {
+        if (nu == mu) continue;
+        int s_nup, s_num, s_diag;
+        if constexpr (sizeof(T) == 4) {
+            const int b_nu = step_offset(g, n, nu, -1);
+            s_nup = (n.lex + step_offset(g, n, nu, +1)) >> 1;
+            s_num = (n.lex + b_nu) >> 1;
+            s_diag = (n.lex + f_mu + b_nu) >> 1;
+        } else {
+            s_nup = lex_step(g, n, nu, +1) >> 1;
+            s_num = lex_step(g, n, nu, -1) >> 1;
+            s_diag = lex_step2(g, n, mu, +1, nu, -1) >> 1;
+        }
+        if (!meas_takes(mu, nu)) {
+            {
+                M3<T> t = mul_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
+                acc_mul_nd(A, t, in.load(nu, p, s));
+            }
+            {
+                M3<T> t = mul_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
+                acc_mul(A, t, in.load(nu, q, s_num));
+            }
+            continue;
+        }
+        // this thread's plane: the staple pieces separately, then W = S_up - S_low
+        M3<T> W;
+        {
+            M3<T> t = mul_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
+            W = mul_nd(t, in.load(nu, p, s));
+        }
+        add_to(A, W);
+        plaq += retr_mul(in.load(mu, p, s), W);  // ReTr(U S_up), the plaquette of the plane at n
+        asm volatile("" ::: "memory");
+        {
+            M3<T> t = mul_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
+            M3<T> S = mul(t, in.load(nu, q, s_num));
+            add_to(A, S);
+            sub_from(W, S);
+        }
+        const bool neg = nu < mu;  // F_numu = -F_munu
+        const int pl = neg ? plane_of(nu, mu) : plane_of(mu, nu);
+        asm volatile("" ::: "memory");
+        cp.ah.store(2 * pl, p, s, ah_neg_if(proj_ah8(mul(in.load(mu, p, s), W)), neg));
+        asm volatile("" ::: "memory");
+        cp.ah.store(2 * pl + 1, q, s_mu, ah_neg_if(proj_ah8(mul(W, in.load(mu, p, s))), neg));
+    }
+    cp.plaq[(mu * 2 + p) * g.Vh + s] = plaq;
+    const M3<T> U = in.load(mu, p, s);
+    const AH8<T> Z = project_ah(mul(U, A));
+    zf.store(mu, p, s, Z);
+    const AH8<T> M = ah_scale(alpha, Z);
+    if (KIND == EXP_MORNINGSTAR) out.store(mu, p, s, mul_plus_right(expm_morningstar<T, true>(M), U));
+    else out.store(mu, p, s, mul(expm<T>(KIND, M), U));
+}
+
+#define GLAC_FLOW_MEAS_KERNEL(NAME, ATTR)                                                                  \
+    template <typename T, int KIND>                                                                      \
+    __global__ void ATTR NAME(Geom g, LinkField<T> in, LinkField<T> out, ForceField<T> zf,               \
+                              CloverParts<T> cp, T alpha) {                                              \
+        flow_stage0_meas_body<T, KIND>(g, in, out, zf, cp, alpha, blockIdx.x);                           \
+    }
+GLAC_FLOW_MEAS_KERNEL(k_flow_stage0_meas, __launch_bounds__(128))
+GLAC_FLOW_MEAS_KERNEL(k_flow_stage0_meas_r128, __maxnreg__(128))
+#undef GLAC_FLOW_MEAS_KERNEL
+
+template <typename T>
+void launch_flow_stage0_meas(const Geom &g, const LinkField<T> &in, const LinkField<T> &out, const ForceField<T> &zf,
+                             const CloverParts<T> &cp, int kind, double alpha, int regs, cudaStream_t st) {
+    const dim3 grid(8 * ((g.Vh + 127) / 128));
+    const T a = (T)alpha;
+#define GLAC_MEAS_CASE(K)                                                                                 \
+    if (kind == K) {                                                                                      \
+        if (regs == 128) k_flow_stage0_meas_r128<T, K><<<grid, 128, 0, st>>>(g, in, out, zf, cp, a);        \
+        else k_flow_stage0_meas<T, K><<<grid, 128, 0, st>>>(g, in, out, zf, cp, a);                       \
+        return;                                                                                           \
+    }
+    GLAC_MEAS_CASE(0) GLAC_MEAS_CASE(1) GLAC_MEAS_CASE(2) GLAC_MEAS_CASE(3)
+#undef GLAC_MEAS_CASE
+    throw std::invalid_argument("bad exp kind");
+}
+template void launch_flow_stage0_meas<double>(const Geom &, const LinkField<double> &, const LinkField<double> &,
+                                              const ForceField<double> &, const CloverParts<double> &, int, double,
+                                              int, cudaStream_t);
+template void launch_flow_stage0_meas<float>(const Geom &, const LinkField<float> &, const LinkField<float> &,
+                                             const ForceField<float> &, const CloverParts<float> &, int, double, int,
+                                             cudaStream_t);
+
+// ---------------------------------------------------------------------------
 // Checkerboard Metropolis sub-sweep over the links (mu, parity p).
 // Staple A once per link, then nhits proposals U' = X U with X = R S T or its
 // inverse (GLAC/math/matrices/su3matrixgenerator.h:170-321), accepted iff
@@ -523,29 +681,6 @@ ObsPlan make_obs_plan(const Geom &g) {
     return pl;
 }
 
-// (C - C^+) made traceless, in the 8-real form: diagonal 2 i Im C_ii minus a
-// third of its trace, off-diagonal C_ij - conj(C_ji).  Linear in C.
-template <typename T> __device__ __forceinline__ AH8<T> proj_ah8(const M3<T> &C) {
-    AH8<T> F;
-    const T two = T(2);
-    const T tr = (C(0, 0).im + C(1, 1).im + C(2, 2).im) * T(2.0 / 3.0);
-    F.a = two * C(0, 0).im - tr;
-    F.d = two * C(1, 1).im - tr;
-    F.b = cx(C(0, 1).re - C(1, 0).re, C(0, 1).im + C(1, 0).im);
-    F.c = cx(C(0, 2).re - C(2, 0).re, C(0, 2).im + C(2, 0).im);
-    F.e = cx(C(1, 2).re - C(2, 1).re, C(1, 2).im + C(2, 1).im);
-    return F;
-}
-template <typename T> __device__ __forceinline__ AH8<T> ah_add(const AH8<T> &X, const AH8<T> &Y) {
-    AH8<T> Z;
-    Z.a = X.a + Y.a;
-    Z.d = X.d + Y.d;
-    Z.b = X.b + Y.b;
-    Z.c = X.c + Y.c;
-    Z.e = X.e + Y.e;
-    return Z;
-}
-
 // Clover of the (mu, nu) plane at n, projected: F = (C - C^+) - 1/3 i ImTr(C - C^+),
 // returned in the 8-real form; *plaq = ReTr(leaf1).  Links are re-read from
 // L1/L2 rather than held, to keep register pressure low.  C = leaf1 - leaf2 +
@@ -658,6 +793,26 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
+// Block sums of the three per-thread values in a fixed order (warp shuffles,
+// then the warps in order) into partial[3 b .. 3 b + 2] = (plaq, energy, q).
+__device__ __forceinline__ void obs_block_reduce(double plaq, double en, double qt, double *partial, int b) {
+    __shared__ double sh[3][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    plaq = warp_sum_d(plaq);
+    en = warp_sum_d(en);
+    qt = warp_sum_d(qt);
+    if (lane == 0) { sh[0][wid] = plaq; sh[1][wid] = en; sh[2][wid] = qt; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double a = 0.0, e = 0.0, q = 0.0;
+        for (int w = 0; w < nw; w++) { a += sh[0][w]; e += sh[1][w]; q += sh[2][w]; }
+        partial[3 * b] = a;
+        partial[3 * b + 1] = e;
+        partial[3 * b + 2] = q;
+    }
+}
+
 // With dq/de set, also the per-site densities in lexicographic order:
 // dq[n] = -(1/(16^2 pi^2)) sum ReTr(C_0nu C_rhosigma), de[n] = sum ReTr(C C) (unnormalised),
 // the fields LatticeActionChargeDensity writes (latticeactionchargedensity.cpp:169-306).
@@ -690,22 +845,7 @@ __device__ __forceinline__ void observables_body(const Geom &g, const LinkField<
             de[n.lex] = en;
         }
     }
-    // deterministic block reduction
-    __shared__ double sh[3][32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    plaq = warp_sum_d(plaq);
-    en = warp_sum_d(en);
-    qt = warp_sum_d(qt);
-    if (lane == 0) { sh[0][wid] = plaq; sh[1][wid] = en; sh[2][wid] = qt; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int nw = (blockDim.x + 31) >> 5;
-        double a = 0.0, e = 0.0, q = 0.0;
-        for (int w = 0; w < nw; w++) { a += sh[0][w]; e += sh[1][w]; q += sh[2][w]; }
-        partial[3 * b] = a;
-        partial[3 * b + 1] = e;
-        partial[3 * b + 2] = q;
-    }
+    obs_block_reduce(plaq, en, qt, partial, b);
 }
 
 #define GLAC_OBS_KERNEL(NAME, ATTR)                                                                      \
@@ -775,6 +915,46 @@ void launch_observables(const Geom &g, const LinkField<T> &L, const ObsPlan &pla
     }
     k_obs_finalize<<<1, 1024, 0, st>>>(g.N[3], plan.nb, g.V, partial, out);
 }
+// The measurement from the parts that flow stage 0 wrote (flow_stage0_meas_body):
+// per site F of each plane = its local + forward slot, the plaquette = the four
+// direction sums; Q(t), E and the plaquette reduced as in observables_body (same
+// blocks, same fixed order), then k_obs_finalize.
+template <typename T>
+__global__ void __launch_bounds__(256) k_obs_combine(Geom g, CloverParts<T> cp, int nb, int Bv, double *partial) {
+    const int b = blockIdx.x;
+    const int t = b / (2 * nb);
+    const int p = (b / nb) & 1;
+    const int j = b % nb;
+    const int half_slice = g.Vh / g.N[3];
+    const bool valid = (int)threadIdx.x < Bv;
+    const int s = t * half_slice + j * Bv + (valid ? (int)threadIdx.x : 0);
+    double plaq = 0.0, en = 0.0, qt = 0.0;
+    if (valid) {
+        AH8<T> F[6];
+#pragma unroll
+        for (int pl = 0; pl < 6; pl++) F[pl] = ah_add(cp.ah.load(2 * pl, p, s), cp.ah.load(2 * pl + 1, p, s));
+#pragma unroll
+        for (int mu = 0; mu < 4; mu++) plaq += (double)cp.plaq[(mu * 2 + p) * g.Vh + s];
+        // q = -[ReTr(F_01 F_23) + ReTr(F_02 F_31) + ReTr(F_03 F_12)], F_31 = -F_13
+        qt = -((double)retr_ah(F[0], F[5]) - (double)retr_ah(F[1], F[4]) + (double)retr_ah(F[2], F[3]));
+#pragma unroll
+        for (int pl = 0; pl < 6; pl++) en += (double)retr_ah(F[pl], F[pl]);
+    }
+    obs_block_reduce(plaq, en, qt, partial, b);
+}
+
+template <typename T>
+void launch_obs_combine(const Geom &g, const CloverParts<T> &cp, const ObsPlan &plan, double *partial, double *out,
+                        cudaStream_t st) {
+    if (g.N[3] > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
+    k_obs_combine<T><<<plan.nblocks, plan.B, 0, st>>>(g, cp, plan.nb, plan.Bv, partial);
+    k_obs_finalize<<<1, 1024, 0, st>>>(g.N[3], plan.nb, g.V, partial, out);
+}
+template void launch_obs_combine<double>(const Geom &, const CloverParts<double> &, const ObsPlan &, double *,
+                                         double *, cudaStream_t);
+template void launch_obs_combine<float>(const Geom &, const CloverParts<float> &, const ObsPlan &, double *, double *,
+                                        cudaStream_t);
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_observables_density(Geom g, LinkField<T> L, int nb, int Bv, double *partial,
                                                              double *dq, double *de) {

@@ -77,6 +77,20 @@ int variant_shape(Family f, bool fp32, int v);  // flow site-block shape of a va
 template <typename T>
 void launch_flow_stage(const Geom &g, const LinkField<T> &in, const LinkField<T> &out, const ForceField<T> &zf,
                        int stage, int kind, double alpha, double beta, int variant, cudaStream_t st);
+// Flow stage 0 that also writes the clover parts of its input field's
+// measurement (regs: 0 = the compiler's allocation, 128 = capped), and the
+// measurement from those parts ([plaq, topc, energy, topct[Nt]] into out).
+template <typename T>
+void launch_flow_stage0_meas(const Geom &g, const LinkField<T> &in, const LinkField<T> &out, const ForceField<T> &zf,
+                             const CloverParts<T> &cp, int kind, double alpha, int regs, cudaStream_t st);
+template <typename T>
+void launch_obs_combine(const Geom &g, const CloverParts<T> &cp, const ObsPlan &plan, double *partial, double *out,
+                        cudaStream_t st);
+// whether the 12 clover-part slots of a lattice fit 32-bit element offsets
+inline bool clover_offsets_fit(long long V, bool fp64) {
+    const long long vh32 = ((V / 2) + 31) / 32 * 32;
+    return (fp64 ? 96 : 48) * vh32 < (1ll << 32);
+}
 // P.net set: the learned spread (learned.cuh) replaces eps per link.
 template <typename T>
 void launch_metropolis(const Geom &g, const LinkField<T> &L, int mu, int p, double beta, double eps, int nhits,

@@ -263,6 +263,16 @@ template <> struct ForceField<float> {
     }
 };
 
+// Clover parts of the measurement fused into flow stage 0: twelve slots of
+// traceless anti-Hermitian 8-real matrices per site (slot 2 pl: plane pl's part
+// from the site's own link, 2 pl + 1: the part from the link at n - mu), laid
+// out as a ForceField whose "direction" index runs over the 12 slots, and the
+// four plaquette sums per site, plaq[(mu * 2 + parity) * Vh + s].
+template <typename T> struct CloverParts {
+    ForceField<T> ah;
+    T *plaq;
+};
+
 // ---------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11)
 // ---------------------------------------------------------------------------

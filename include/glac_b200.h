@@ -80,7 +80,14 @@ uint64_t glac_launch_count(const glac_ctx *ctx);
  *   the reference does, x0 = sign(u0) sqrt(1 - eps^2)
  *   (su3matrixgenerator.h:202-243); 0 keeps x0 = +sqrt(1 - eps^2), every factor
  *   near the identity (a symmetric proposal as well; no reference counterpart).
- *   Applies to glac_metropolis and glac_esj_data. */
+ *   Applies to glac_metropolis and glac_esj_data.
+ *   "fused_measure": 1 or 2 (default 2 in FP32, 1 in FP64): glac_flow
+ *   measures the field before each step inside that step's first RK3 stage,
+ *   from the staple pieces the stage computes anyway (two extra 3x3 products
+ *   per plane instead of the ten of a separate clover pass), and the last one
+ *   in a pass of its own; 1 uses the stage kernel's own register allocation, 2
+ *   a 128-register variant; 0 measures every field in a pass of its own.  The
+ *   results are the same to rounding. */
 glac_status glac_set_option(glac_ctx *ctx, const char *key, long value);
 
 /* ---- field --------------------------------------------------------------- */

@@ -211,14 +211,46 @@ def test_flow_variants_agree(g, oracle, prec):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("N", [(6, 4, 6, 8), (8, 8, 8, 16)])
+def test_measurement_inside_flow_stage0(g, oracle, prec, N):
+    # glac_flow measures the field before each step inside that step's stage 0
+    # (the clover from the staple pieces, combined per site afterwards); with
+    # fused_measure = 0 every field is measured by the stand-alone pass.  On the
+    # oracle's own flowed fields (set before each one-step flow, so both
+    # measure exactly the same field): fused, stand-alone and oracle agree to
+    # the bar, and both modes flow the field the same.
+    with lattice(g, N, "fp64", beta=6.0, seed=77) as C:
+        C.set_links(oracle.haar_field(N, 77))
+        C.metropolis(10)
+        cur = C.get_links()
+    with lattice(g, N, prec, flow_eps=0.02) as A, lattice(g, N, prec, flow_eps=0.02) as B:
+        B.set_option("fused_measure", 0)
+        for k in range(4):
+            A.set_links(cur)
+            B.set_links(cur)
+            oa, ob = A.flow(1), B.flow(1)
+            want = oracle.observables(N, cur)
+            assert_obs_close(oa[0], want, TOL[prec], f"fused, field {k}")
+            assert_obs_close(ob[0], want, TOL[prec], f"stand-alone, field {k}")
+            assert_obs_close(oa, ob, TOL[prec], f"fused vs stand-alone, field {k}")
+            nxt = oracle.flow(N, cur, 0.02, 1)
+            assert rel_err(A.get_links(), nxt) < TOL[prec] and rel_err(B.get_links(), nxt) < TOL[prec]
+            cur = nxt
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_flow_vs_live_reference_larger(g, oracle, reference, prec):
-    # Step by step from a Haar field (the roughest input) at eps = 0.02: after
-    # step k the field and the observables within k times the one-step bar,
-    # since each step adds its own rounding differences (FP64 on B200: 3e-13
-    # per step in the links, 1.1e-12 after four steps).
+    # Step by step at eps = 0.02 from a field 20 FP64 sweeps away from a Haar
+    # start (plaquette ~0.5; the plaquette of the Haar field itself is ~0, where a
+    # relative error says nothing): after step k the field and the observables
+    # within k times the one-step bar, since each step adds its own rounding
+    # differences (FP64 on B200: ~3e-13 per step in the links).
     N = (8, 8, 8, 8)
     reference.configure(8, 8, flow_eps=0.02, nflows=4)
-    links = oracle.haar_field(N, 4242)
+    with lattice(g, N, "fp64", beta=6.0, seed=4242) as C:
+        C.set_links(oracle.haar_field(N, 4242))
+        C.metropolis(20)
+        links = C.get_links()
     with lattice(g, N, prec, flow_eps=0.02) as L:
         L.set_links(links)
         cur = links
