@@ -12,6 +12,11 @@ primary observable:
 * bias correction of Gamma by C_F(W)/N, error of tau_int from the Madras-Sokal
   formula d tau ~= tau * sqrt((4W + 2)/N), error of the mean sqrt(C_F/N).
 
+For several independent chains (replicas) of one algorithm, Wolff Section 3.3:
+Gamma(t) is averaged over the replicas about the grand mean, with N the total
+number of samples (gamma_method_replicas), and a delete-one-replica jackknife
+gives errors of derived quantities (jackknife).
+
 Also binned (jackknife-free) errors for several chains, used when chains are
 short compared with their autocorrelation.
 """
@@ -46,6 +51,67 @@ def autocorrelation(a: np.ndarray) -> np.ndarray:
     f = np.fft.rfft(d, m)
     g = np.fft.irfft(f * np.conj(f), m)[:n]
     return g / (n - np.arange(n))
+
+
+def _window(G: np.ndarray, n: int, S: float) -> int:
+    """Wolff's automatic window for the autocorrelation function G of n samples."""
+    wmax = G.size - 1
+    tint = 0.5
+    for w in range(1, wmax + 1):
+        tint += G[w] / G[0]
+        if tint <= 0.5:
+            tau = 1e-12  # decorrelated faster than a step: stop at once
+        else:
+            tau = S / np.log((2 * tint + 1) / (2 * tint - 1))
+        if np.exp(-w / tau) - tau / np.sqrt(w * n) < 0:
+            return w
+    return wmax
+
+
+def gamma_method_replicas(chains, S: float = 1.5) -> GammaResult:
+    """The Gamma method for R independent replicas of one chain (Wolff, Section 3.3).
+
+    Gamma(t) = sum_r sum_i (a_ri - abar)(a_r,i+t - abar) / sum_r (N_r - t),
+    abar the grand mean; window, bias correction and errors as in
+    gamma_method with N = sum_r N_r.  (The mean over replicas of unequal
+    length is weighted by N_r.)
+    """
+    chains = [np.asarray(c, np.float64).ravel() for c in chains]
+    if len(chains) == 1:
+        return gamma_method(chains[0], S)
+    n = sum(c.size for c in chains)
+    if min(c.size for c in chains) < 4:
+        raise ValueError("every replica needs at least 4 samples")
+    abar = float(sum(c.sum() for c in chains) / n)
+    tmax = min(c.size for c in chains) // 2
+    num = np.zeros(tmax + 1)
+    den = np.zeros(tmax + 1)
+    for c in chains:
+        d = c - abar
+        m = 1 << (2 * d.size - 1).bit_length()
+        f = np.fft.rfft(d, m)
+        g = np.fft.irfft(f * np.conj(f), m)[:tmax + 1]
+        num += g
+        den += d.size - np.arange(tmax + 1)
+    G = num / den
+    if G[0] <= 0.0:
+        return GammaResult(abar, 0.0, 0.5, 0.0, 0, n)
+    W = _window(G, n, S)
+    CF = G[0] + 2.0 * G[1:W + 1].sum()
+    Gc = G[:W + 1] + CF / n
+    CF = Gc[0] + 2.0 * Gc[1:].sum()
+    tau_int = max(CF / (2.0 * Gc[0]), 0.5)
+    tau_err = tau_int * np.sqrt((4.0 * W + 2.0) / n)
+    return GammaResult(abar, float(np.sqrt(max(CF, 0.0) / n)), float(tau_int), float(tau_err), int(W), n)
+
+
+def jackknife(values_by_replica_removed):
+    """Jackknife error from the R delete-one-replica estimates of a quantity."""
+    v = np.asarray(values_by_replica_removed, np.float64)
+    R = v.size
+    if R < 2:
+        return float("nan")
+    return float(np.sqrt((R - 1) / R * np.sum((v - v.mean()) ** 2)))
 
 
 def gamma_method(a, S: float = 1.5) -> GammaResult:

@@ -5,6 +5,18 @@
     (link-updates/s), FP32 and FP64 flow with per-step observables (site-steps/s),
     the HBM GB/s of the flow stage, and one full flow to t = 4 (400 RK3 steps).
 
+``python -m glac_b200.studies target [--replicas 0,1,2,3] [--samplers ...] [--out f.json]``
+``python -m glac_b200.studies target-combine f1.json f2.json ...``
+    The effective-topological-charge study at 32^3 x 64, beta = 6.2: from
+    independently thermalised starts (one per replica), chains of the plain
+    FP64 sampler (the reference's proposal, SU3Eps = 0.24), the plain FP32
+    sampler, the FP32 sampler with the no-flip proposal family at its best fixed
+    spread (the ablation) and the FP32 learned-spread sampler; Q and E at flow
+    time t and the plaquette every `meas_every` sweeps; effective Q samples per
+    second = N_meas / (2 tau_int,Q) / wall seconds (sweeps and measurements),
+    tau_int by the replica Gamma method, errors by a delete-one-replica
+    jackknife.  Replicas can be run in separate processes and combined.
+
 ``python -m glac_b200.studies precision [--dims 32,32,32,64] [--steps 1000]``
     Flow-only precision test: a start field from plain FP64 Metropolis sweeps
     (seeded Haar start), flowed with Luescher RK3 (Morningstar-Peardon
@@ -138,6 +150,163 @@ def large_run(dims=(48, 48, 48, 96), beta=6.45, therm=200, seed=20261203, flow_s
     return out
 
 
+# ---------------------------------------------------------------------------
+# effective topological-charge samples per second at the target configuration
+# ---------------------------------------------------------------------------
+TARGET = dict(dims=(32, 32, 32, 64), beta=6.2, therm=3000, sweeps=20000, meas_every=50, flow_eps=0.04,
+              flow_t=2.0, train_therm=1000, train_sweeps=400, train_every=20, seed=20261203)
+SAMPLERS = ("plain_fp64", "plain_fp32", "ablation_fp32", "learned_fp32")
+
+
+def target_training(cfg=TARGET):
+    """Train the spread network on ESJ data of the plain FP32 sampler at the
+    target coupling; returns (params, training report)."""
+    from . import learned as lp
+    dims, beta, seed = tuple(cfg["dims"]), cfg["beta"], cfg["seed"]
+    with Lattice(dims, beta=beta, precision="fp32", seed=seed, stream_id=999, reunit_interval=10) as L:
+        L.hot_start(seed + 999)
+        L.set_option("su2_sign_flips", 0)
+        L.metropolis(cfg["train_therm"])
+        L.set_option("su2_sign_flips", 1)
+        feat, esj, plain = lp.collect_esj(L, cfg["train_sweeps"], cfg["train_every"], 64, lp.DEFAULT_GRID, trials=4)
+    net, rep = lp.train_proposal(feat, esj, lp.DEFAULT_GRID, steps=3000, seed=seed, esj_plain=plain)
+    params = net.params
+    net.close()
+    return params, rep
+
+
+def target_start(cfg, replica, params=None, best_eps=0.36):
+    """Replica `replica`'s start: its own Haar field thermalised by cfg["therm"]
+    sweeps of the no-flip FP32 sampler at best_eps (reunitarised every 10)."""
+    dims, beta, seed = tuple(cfg["dims"]), cfg["beta"], cfg["seed"]
+    with Lattice(dims, beta=beta, precision="fp32", su3_eps=best_eps, seed=seed, stream_id=1000 + replica,
+                 reunit_interval=10) as L:
+        L.hot_start(seed + 7919 * (replica + 1))
+        L.set_option("su2_sign_flips", 0)
+        L.metropolis(cfg["therm"])
+        L.reunitarize()
+        return L.get_links()
+
+
+def q_chain(start, cfg, sampler, replica, params=None, best_eps=0.36):
+    """One chain of `sampler` from `start`; every meas_every sweeps the plaquette
+    of the chain and Q, E of a flowed copy at t = flow_t.  Wall seconds cover the
+    sweeps and the measurements (device synchronised at both ends)."""
+    from .learned import DEFAULT_GRID
+    dims, beta, seed = tuple(cfg["dims"]), cfg["beta"], cfg["seed"]
+    prec = "fp64" if sampler.endswith("fp64") else "fp32"
+    flips = sampler.startswith("plain")
+    eps = best_eps if sampler.startswith("ablation") else 0.24
+    stream = 10 * replica + SAMPLERS.index(sampler)
+    fs = int(round(cfg["flow_t"] / cfg["flow_eps"]))
+    nmeas = cfg["sweeps"] // cfg["meas_every"]
+    plaq, Q, E = np.empty(nmeas), np.empty(nmeas), np.empty(nmeas)
+    acc = 0.0
+    with Lattice(dims, beta=beta, precision=prec, su3_eps=eps, seed=seed, stream_id=stream,
+                 reunit_interval=10 if prec == "fp32" else 0) as L, \
+            Lattice(dims, beta=beta, precision=prec, flow_eps=cfg["flow_eps"], seed=seed) as F:
+        L.set_links(start)
+        L.set_option("su2_sign_flips", int(flips))
+        if sampler.startswith("learned"):
+            L.set_proposal_net(params, float(DEFAULT_GRID[0]), float(DEFAULT_GRID[-1]))
+        L.autotune(2)  # launch variants (field and random stream restored)
+        F.set_links(start)
+        F.autotune(2)
+        L.sync()
+        F.sync()
+        t0 = time.perf_counter()
+        for i in range(nmeas):
+            acc += L.metropolis(cfg["meas_every"])
+            plaq[i] = L.measure()[0]
+            F.copy_from(L)
+            F.flow(fs, measure=False)
+            o = F.measure()
+            Q[i], E[i] = o[1], o[2]
+        F.sync()
+        wall = time.perf_counter() - t0
+    return dict(sampler=sampler, replica=replica, precision=prec, su3_eps=None if sampler.startswith("learned") else eps,
+                su2_sign_flips=flips, sweeps=cfg["sweeps"], meas_every=cfg["meas_every"], wall_s=wall,
+                acceptance=acc / nmeas, plaq=plaq.tolist(), Q=Q.tolist(), E=E.tolist())
+
+
+def target_run(replicas, samplers=SAMPLERS, cfg=TARGET, params=None):
+    """Chains of the given samplers for the given replicas (training first when
+    params is None); a JSON-able dict that target_combine merges."""
+    out = dict(config={k: (list(v) if isinstance(v, tuple) else v) for k, v in cfg.items()}, chains=[])
+    if params is None:
+        params, rep = target_training(cfg)
+        out["training"] = rep
+    else:
+        rep = None
+    params = np.asarray(params, np.float32)
+    best = float(rep["best_fixed_eps"]) if rep else float(cfg.get("best_eps", 0.36))
+    out["params"] = [float(x) for x in params]
+    out["best_eps"] = best
+    for r in replicas:
+        t0 = time.time()
+        start = target_start(cfg, r, params, best)
+        therm_s = time.time() - t0
+        for smp in samplers:
+            c = q_chain(start, cfg, smp, r, params, best)
+            c["therm_seconds"] = therm_s
+            out["chains"].append(c)
+    return out
+
+
+def target_combine(runs):
+    """Per sampler: tau_int of Q and of the plaquette (replica Gamma method),
+    effective Q samples per second, means; ratios to plain FP64 with
+    delete-one-replica jackknife errors.  tau_int,Q of the plain FP64 sampler
+    is also given from its FP32 twin (the same Markov kernel up to rounding),
+    pooled with it when both ran."""
+    from .analysis import gamma_method_replicas, jackknife
+    chains = [c for r in runs for c in r["chains"]]
+    by = {}
+    for c in chains:
+        by.setdefault(c["sampler"], {})[c["replica"]] = c
+    res = {}
+
+    def stats(cs):
+        tq = gamma_method_replicas([c["Q"] for c in cs])
+        tp = gamma_method_replicas([c["plaq"] for c in cs])
+        q2 = gamma_method_replicas([np.square(c["Q"]) for c in cs])
+        te = gamma_method_replicas([c["E"] for c in cs])
+        nmeas = sum(len(c["Q"]) for c in cs)
+        wall = sum(c["wall_s"] for c in cs)
+        return dict(tau_Q=tq.tau_int * cs[0]["meas_every"], tau_Q_err=tq.tau_error * cs[0]["meas_every"],
+                    tau_plaq=tp.tau_int * cs[0]["meas_every"], plaq=tp.mean, plaq_err=tp.error,
+                    Q2=q2.mean, Q2_err=q2.error, E=te.mean, E_err=te.error, n_meas=nmeas, wall_s=wall,
+                    sweep_seconds=wall / sum(c["sweeps"] for c in cs),
+                    eff_Q_per_s=nmeas / (2.0 * tq.tau_int) / wall, replicas=sorted(c["replica"] for c in cs),
+                    acceptance=float(np.mean([c["acceptance"] for c in cs])))
+
+    for smp, reps in by.items():
+        res[smp] = stats(list(reps.values()))
+    common = sorted(set.intersection(*[set(v) for v in by.values()])) if by else []
+    base = "plain_fp64" if "plain_fp64" in res else None
+    if base:
+        for smp in res:
+            res[smp]["eff_Q_ratio_vs_plain_fp64"] = res[smp]["eff_Q_per_s"] / res[base]["eff_Q_per_s"]
+            if len(common) >= 2:
+                loo = []
+                for k in common:
+                    keep = [r for r in common if r != k]
+                    a = stats([by[smp][r] for r in keep])
+                    b = stats([by[base][r] for r in keep])
+                    loo.append(a["eff_Q_per_s"] / b["eff_Q_per_s"])
+                res[smp]["eff_Q_ratio_err"] = jackknife(loo)
+    if "plain_fp32" in res and "plain_fp64" in res:
+        # FP64 rate with the pooled tau_int,Q of the plain kernel (FP32 and FP64 chains)
+        pooled = gamma_method_replicas([c["Q"] for s in ("plain_fp32", "plain_fp64") for c in by[s].values()])
+        f64 = res["plain_fp64"]
+        f64["tau_Q_pooled_plain"] = pooled.tau_int * chains[0]["meas_every"]
+        f64["eff_Q_per_s_pooled_tau"] = f64["n_meas"] / (2.0 * pooled.tau_int) / f64["wall_s"]
+        for smp in res:
+            res[smp]["eff_Q_ratio_vs_plain_fp64_pooled_tau"] = res[smp]["eff_Q_per_s"] / f64["eff_Q_per_s_pooled_tau"]
+    return dict(config=runs[0]["config"], best_eps=runs[0].get("best_eps"), samplers=res,
+                training=next((r["training"] for r in runs if r.get("training")), None))
+
+
 def _main():
     ap = argparse.ArgumentParser(prog="python -m glac_b200.studies")
     sub = ap.add_subparsers(dest="study", required=True)
@@ -152,7 +321,40 @@ def _main():
     q.add_argument("--dims", default="48,48,48,96")
     q.add_argument("--beta", type=float, default=6.45)
     q.add_argument("--therm", type=int, default=200)
+    t = sub.add_parser("target", help="effective Q samples/s at 32^3x64, beta=6.2, per sampler")
+    t.add_argument("--replicas", default="0,1,2,3")
+    t.add_argument("--samplers", default=",".join(SAMPLERS))
+    t.add_argument("--sweeps", type=int, default=TARGET["sweeps"])
+    t.add_argument("--meas-every", type=int, default=TARGET["meas_every"])
+    t.add_argument("--therm", type=int, default=TARGET["therm"])
+    t.add_argument("--dims", default="32,32,32,64")
+    t.add_argument("--params", default="", help="JSON of an earlier run whose trained network to reuse")
+    t.add_argument("--out", default="")
+    c = sub.add_parser("target-combine", help="merge target runs and print the summary")
+    c.add_argument("files", nargs="+")
     a = ap.parse_args()
+    if a.study == "target":
+        cfg = dict(TARGET, sweeps=a.sweeps, meas_every=a.meas_every, therm=a.therm,
+                   dims=tuple(int(x) for x in a.dims.split(",")))
+        params = None
+        if a.params:
+            with open(a.params) as f:
+                prev = json.load(f)
+            params = prev["params"]
+            cfg["best_eps"] = prev["best_eps"]
+        r = target_run([int(x) for x in a.replicas.split(",")], a.samplers.split(","), cfg, params)
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(r, f)
+        print(json.dumps(target_combine([r])["samplers"]))
+        return
+    if a.study == "target-combine":
+        runs = []
+        for fn in a.files:
+            with open(fn) as f:
+                runs.append(json.load(f))
+        print(json.dumps(target_combine(runs), indent=1))
+        return
     if a.study == "large":
         print(json.dumps(large_run(tuple(int(x) for x in a.dims.split(",")), a.beta, a.therm)))
         return

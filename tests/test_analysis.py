@@ -30,3 +30,20 @@ def test_constant_series_and_bins():
     assert m == pytest.approx(49.5) and e > 0
     with pytest.raises(ValueError):
         gamma_method([1.0, 2.0])
+
+
+def test_replica_gamma_method_on_ar1():
+    # four independent AR(1) replicas: the pooled estimate finds the known tau_int
+    from glac_b200.analysis import gamma_method_replicas, jackknife
+    rho = 0.8
+    chains = [ar1(20_000, rho, seed=10 + r) for r in range(4)]
+    r = gamma_method_replicas(chains)
+    want = (1 + rho) / (2 * (1 - rho))
+    assert r.n == 80_000
+    assert abs(r.tau_int - want) < 4 * r.tau_error
+    # delete-one-replica jackknife of tau_int: an error of the size Madras-Sokal gives
+    loo = [gamma_method_replicas(chains[:k] + chains[k + 1:]).tau_int for k in range(4)]
+    je = jackknife(loo)
+    assert 0.2 * r.tau_error < je < 5 * r.tau_error
+    # one replica: the single-chain method
+    assert gamma_method_replicas(chains[:1]).tau_int == gamma_method(chains[0]).tau_int
