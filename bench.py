@@ -49,6 +49,10 @@ WORKLOAD = "GLAC gradient flow 32^3x64, beta=6.2, eps=0.01, FP32 links + FP64 su
 STAGE_BYTES_FP32 = (8 * 72 + 4 * 32, 8 * 72 + 8 * 32, 8 * 72 + 4 * 32)
 STAGE_BYTES_FP64 = tuple(2 * b for b in STAGE_BYTES_FP32)
 NCU_TRAFFIC_STAGE0_FP32 = 636109568 + 837838592  # bytes, one ncu capture of the launch (uncapped variant)
+# stage 0 with the measurement's clover parts: + 12 slots x 32 B + 4 plaquette floats per site written
+STAGE0_MEAS_BYTES_FP32 = STAGE_BYTES_FP32[0] + 12 * 32 + 4 * 4
+NCU_TRAFFIC_STAGE0_MEAS_FP32 = None  # bytes per launch from an ncu capture at 32^3x64 (profiles/)
+FLOPS_PER_SITE_STAGE0_MEAS_FP32 = None  # from ncu instruction counts of that launch (profiles/)
 # FP32 floating-point operations per site of one stage-0 launch: 4 links x
 # (2 x FFMA + FADD + FMUL) thread instructions counted by ncu
 # (sm__sass_thread_inst_executed_op_{ffma,fadd,fmul}_pred_on) on the 32^3x64 launch
@@ -342,35 +346,49 @@ def run_gpu(args):
 
     # roofline of the flow-stage kernel: CUDA events around each stage launch on
     # the lattice's stream, averaged over reps RK3 steps
+    # roofline of the dominant kernel of the timed region: flow stage 0 with the
+    # measurement's clover parts (k_flow_stage0_meas); CUDA events around each
+    # launch of measured flow steps on the lattice's stream, right after the
+    # timed region, with the SM clock sampled meanwhile
     reps = max(3, min(args.steps, 20))
     clk_st = ClockSampler(local)
     clk_st.start()
+    stm = np.array(L.flow_stage_times_measured(reps))
     st = np.array(L.flow_stage_times(reps))
     stage_clocks = clk_st.stop()
     hbm_peak, peak_kind = load_peaks()
-    # dominant kernel: the stage-0 flow launch; algorithmic bytes = 4 links read
-    # + 4 links written + force written per site (704 B FP32)
-    alg_bytes = STAGE_BYTES_FP32[0] * V
-    achieved = alg_bytes / float(st[0]) / 1e9
+    alg_bytes = STAGE0_MEAS_BYTES_FP32 * V
+    achieved = alg_bytes / float(stm[0]) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(achieved / hbm_peak, 4),
                 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of
                 # this launch at 32^3x64
-                "traffic": NCU_TRAFFIC_STAGE0_FP32 if DIMS == (32, 32, 32, 64) else None,
-                "kernel": "k_flow_stage<float, morningstar, stage 0>",
+                "traffic": NCU_TRAFFIC_STAGE0_MEAS_FP32 if DIMS == (32, 32, 32, 64) else None,
+                "kernel": "k_flow_stage0_meas_r128<float, morningstar>",
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind,
-                "stage_ms": [round(x * 1e3, 4) for x in st],
-                "stage_ms_how": (f"CUDA events around each stage launch over {reps} RK3 steps right after the timed "
+                "measured_step_ms": {"stage0_with_clover_parts": round(stm[0] * 1e3, 4),
+                                     "measurement_combine_and_reduce": round(stm[1] * 1e3, 4),
+                                     "stage1": round(stm[2] * 1e3, 4), "stage2": round(stm[3] * 1e3, 4)},
+                "unmeasured_stage_ms": [round(x * 1e3, 4) for x in st],
+                "stage_ms_how": (f"CUDA events around each launch over {reps} RK3 steps right after the timed "
                                  f"region; SM clock median {stage_clocks.get('sm_mhz')} MHz meanwhile"),
-                "binding_unit": "FP32 FMA pipe (60 % busy per ncu; HBM 25 %)"}
+                "binding_unit": "FP32 FMA pipe (see profiles/)"}
     # the binding unit: FP32 FLOP/s of the same launch against the FP32 peak at the
-    # median SM clock sampled during the timed region (148 SMs x 128 lanes x 2 FLOP per FMA)
-    sm_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    # median SM clock sampled while it ran (148 SMs x 128 lanes x 2 FLOP per FMA)
+    sm_mhz = stage_clocks.get("sm_mhz") or clocks.get("sm_mhz") or 1965.0
     fp32_peak = SM_COUNT * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
-    fp32_ach = FLOPS_PER_SITE_STAGE0_FP32 * V / float(st[0]) / 1e12
-    roofline["fp32_pipe"] = {"achieved": round(fp32_ach, 2), "peak": round(fp32_peak, 2), "unit": "TFLOP/s",
-                             "frac": round(fp32_ach / fp32_peak, 4), "flops_per_site": FLOPS_PER_SITE_STAGE0_FP32,
-                             "peak_basis": f"148 SMs x 128 FP32 lanes x 2 FLOP x {sm_mhz:.0f} MHz (median under load)"}
+    if FLOPS_PER_SITE_STAGE0_MEAS_FP32:
+        fp32_ach = FLOPS_PER_SITE_STAGE0_MEAS_FP32 * V / float(stm[0]) / 1e12
+        roofline["fp32_pipe"] = {"achieved": round(fp32_ach, 2), "peak": round(fp32_peak, 2), "unit": "TFLOP/s",
+                                 "frac": round(fp32_ach / fp32_peak, 4),
+                                 "flops_per_site": FLOPS_PER_SITE_STAGE0_MEAS_FP32,
+                                 "peak_basis": f"148 SMs x 128 FP32 lanes x 2 FLOP x {sm_mhz:.0f} MHz (median while timed)"}
+    # the plain stage-0 launch (flow steps without measurement) for comparison
+    plain_fp32 = FLOPS_PER_SITE_STAGE0_FP32 * V / float(st[0]) / 1e12
+    roofline["unmeasured_stage0"] = {
+        "kernel": "k_flow_stage<float, morningstar, stage 0>", "ms": round(st[0] * 1e3, 4),
+        "achieved_GBps": round(STAGE_BYTES_FP32[0] * V / float(st[0]) / 1e9, 1),
+        "fp32_pipe_frac": round(plain_fp32 / fp32_peak, 4), "flops_per_site": FLOPS_PER_SITE_STAGE0_FP32}
 
     # FP64 flow for comparison (same field)
     L64 = g.Lattice(DIMS, beta=BETA, precision="fp64", flow_eps=FLOW_EPS, seed=1, stream_id=rank, device=local)

@@ -102,6 +102,7 @@ def lib() -> C.CDLL:
     L.glac_measure.argtypes = [P, C.c_void_p]
     L.glac_flow_configuration.argtypes = [P, C.c_void_p, C.c_int, C.c_void_p]
     L.glac_flow_stage_times.argtypes = [P, C.c_int, _dp]
+    L.glac_flow_stage_times_measured.argtypes = [P, C.c_int, _dp]
     L.glac_autotune.argtypes = [P, C.c_int, C.c_void_p]
     L.glac_get_tuning.argtypes = [P, C.c_void_p]
     L.glac_set_tuning.argtypes = [P, C.c_void_p]
@@ -295,6 +296,13 @@ class Lattice:
         self._ck(lib().glac_flow_stage_times(self._ctx, int(n_steps), out))
         return out
 
+    def flow_stage_times_measured(self, n_steps: int):
+        """Seconds per launch of [stage 0 with the clover parts, the measurement's
+        reduction, stage 1, stage 2] over n_steps measured flow steps."""
+        out = np.zeros(4)
+        self._ck(lib().glac_flow_stage_times_measured(self._ctx, int(n_steps), out))
+        return out
+
     def flow_configuration_ptr(self, host_ptr: int, n_steps: int, obs_ptr: int):
         self._ck(lib().glac_flow_configuration(self._ctx, C.c_void_p(host_ptr), int(n_steps), C.c_void_p(obs_ptr)))
 
@@ -420,15 +428,6 @@ def write_field(path, dims, links):
         raise GlacError(st, lib().glac_io_error().decode())
 
 
-from .reference_api import (  # noqa: E402  (names of the reference's interface)
-    Flow,
-    MasterSamplerTopcXYZ,
-    Plaquette,
-    SU3Exp,
-    WilsonGaugeAction,
-)
-
 __all__ = [
     "Lattice", "exp_batch", "delta_s_batch", "accept_fed", "read_field", "write_field", "build", "lib", "GlacError",
-    "WilsonGaugeAction", "Flow", "SU3Exp", "MasterSamplerTopcXYZ", "Plaquette",
 ]

@@ -164,7 +164,8 @@ void reunit(glac_ctx *c) {
 }
 
 // One Luscher RK3 step: three fused stages, cur -> other -> cur -> other.
-// ev (optional) receives 4 events around the three stage launches.  meas_out
+// ev (optional) receives 4 events around the three stage launches, 5 with
+// meas_out (the fourth after the measurement's reduction).  meas_out
 // (optional, device): the observables of the field before the step, measured
 // inside stage 0 (clover parts) and reduced right after it.
 void flow_step(glac_ctx *c, cudaEvent_t *ev = nullptr, double *meas_out = nullptr) {
@@ -172,6 +173,7 @@ void flow_step(glac_ctx *c, cudaEvent_t *ev = nullptr, double *meas_out = nullpt
     const double alpha[3] = {eps * 0.25, eps * 0.8888888888888888, 0.75 * eps};
     const double beta[3] = {0.0, -(eps * 0.4722222222222222), -1.0};
     if (ev) ck(cudaEventRecord(ev[0], c->stream), "event");
+    int e = 1;
     for (int stage = 0; stage < 3; stage++) {
         const int src = c->cur, dst = c->cur ^ 1;
         if (stage == 0 && meas_out) {
@@ -182,12 +184,14 @@ void flow_step(glac_ctx *c, cudaEvent_t *ev = nullptr, double *meas_out = nullpt
                 launch_flow_stage0_meas(c->g, f64(c, src), f64(c, dst), z64(c), cp, c->d.exp_func, alpha[0], regs,
                                         c->stream);
                 ck_launch("flow stage 0 with measurement");
+                if (ev) ck(cudaEventRecord(ev[e++], c->stream), "event");
                 launch_obs_combine(c->g, cp, c->plan, c->partial, meas_out, c->stream);
             } else {
                 const CloverParts<float> cp = clover_view<float>(c);
                 launch_flow_stage0_meas(c->g, f32(c, src), f32(c, dst), z32(c), cp, c->d.exp_func, alpha[0], regs,
                                         c->stream);
                 ck_launch("flow stage 0 with measurement");
+                if (ev) ck(cudaEventRecord(ev[e++], c->stream), "event");
                 launch_obs_combine(c->g, cp, c->plan, c->partial, meas_out, c->stream);
             }
             ck_launch("measurement from clover parts");
@@ -203,7 +207,7 @@ void flow_step(glac_ctx *c, cudaEvent_t *ev = nullptr, double *meas_out = nullpt
             c->launches += 1;
         }
         c->cur = dst;
-        if (ev) ck(cudaEventRecord(ev[stage + 1], c->stream), "event");
+        if (ev) ck(cudaEventRecord(ev[e++], c->stream), "event");
     }
 }
 
@@ -607,6 +611,36 @@ glac_status glac_flow_stage_times(glac_ctx *c, int n_steps, double *seconds3) {
         }
         for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
         for (int i = 0; i < 3; i++) seconds3[i] = acc[i] / n_steps;
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_flow_stage_times_measured(glac_ctx *c, int n_steps, double *seconds4) {
+    return guarded(c, [&] {
+        glac_status s = need_field(c);
+        if (s != GLAC_OK) return s;
+        if (n_steps <= 0 || !seconds4) { c->err = "n_steps must be > 0"; return GLAC_ERR_ARG; }
+        if (!fused_measure_usable(c)) {
+            c->err = "the measurement is not fused into flow stage 0 for this context (fused_measure = 0, or the "
+                     "lattice is too large for the clover parts' 32-bit offsets)";
+            return GLAC_ERR_STATE;
+        }
+        const size_t per = 3 + (size_t)c->g.N[3];
+        ensure_obs(c, per);
+        cudaEvent_t ev[5];
+        for (int i = 0; i < 5; i++) ck(cudaEventCreate(&ev[i]), "event create");
+        double acc[4] = {0, 0, 0, 0};
+        for (int k = 0; k < n_steps; k++) {
+            flow_step(c, ev, c->obs_dev);
+            ck(cudaEventSynchronize(ev[4]), "event sync");
+            for (int i = 0; i < 4; i++) {
+                float ms = 0.f;
+                ck(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "elapsed");
+                acc[i] += ms * 1e-3;
+            }
+        }
+        for (int i = 0; i < 5; i++) cudaEventDestroy(ev[i]);
+        for (int i = 0; i < 4; i++) seconds4[i] = acc[i] / n_steps;
         return GLAC_OK;
     });
 }

@@ -153,8 +153,13 @@ def large_run(dims=(48, 48, 48, 96), beta=6.45, therm=200, seed=20261203, flow_s
 # ---------------------------------------------------------------------------
 # effective topological-charge samples per second at the target configuration
 # ---------------------------------------------------------------------------
-TARGET = dict(dims=(32, 32, 32, 64), beta=6.2, therm=3000, sweeps=20000, meas_every=50, flow_eps=0.04,
-              flow_t=2.0, train_therm=1000, train_sweeps=400, train_every=20, seed=20261203)
+TARGET = dict(dims=(32, 32, 32, 64), beta=6.2, therm=3000, sweeps=30000, meas_every=100, flow_eps=0.04,
+              flow_t=2.0, train_therm=1000, train_sweeps=400, train_every=20, seed=20261203,
+              # chain length per sampler: the plain kernel decorrelates Q slowest
+              # (tau_int,Q ~ 1000 sweeps at 32^3 x 64, beta = 6.2), the FP64 chains
+              # give its FP64 wall time and a consistency check of the FP32 twin
+              sweeps_by={"plain_fp64": 10000, "plain_fp32": 60000, "ablation_fp32": 30000,
+                         "learned_fp32": 30000})
 SAMPLERS = ("plain_fp64", "plain_fp32", "ablation_fp32", "learned_fp32")
 
 
@@ -199,7 +204,8 @@ def q_chain(start, cfg, sampler, replica, params=None, best_eps=0.36):
     eps = best_eps if sampler.startswith("ablation") else 0.24
     stream = 10 * replica + SAMPLERS.index(sampler)
     fs = int(round(cfg["flow_t"] / cfg["flow_eps"]))
-    nmeas = cfg["sweeps"] // cfg["meas_every"]
+    sweeps = int(cfg.get("sweeps_by", {}).get(sampler, cfg["sweeps"]))
+    nmeas = sweeps // cfg["meas_every"]
     plaq, Q, E = np.empty(nmeas), np.empty(nmeas), np.empty(nmeas)
     acc = 0.0
     with Lattice(dims, beta=beta, precision=prec, su3_eps=eps, seed=seed, stream_id=stream,
@@ -225,13 +231,14 @@ def q_chain(start, cfg, sampler, replica, params=None, best_eps=0.36):
         F.sync()
         wall = time.perf_counter() - t0
     return dict(sampler=sampler, replica=replica, precision=prec, su3_eps=None if sampler.startswith("learned") else eps,
-                su2_sign_flips=flips, sweeps=cfg["sweeps"], meas_every=cfg["meas_every"], wall_s=wall,
+                su2_sign_flips=flips, sweeps=nmeas * cfg["meas_every"], meas_every=cfg["meas_every"], wall_s=wall,
                 acceptance=acc / nmeas, plaq=plaq.tolist(), Q=Q.tolist(), E=E.tolist())
 
 
-def target_run(replicas, samplers=SAMPLERS, cfg=TARGET, params=None):
+def target_run(replicas, samplers=SAMPLERS, cfg=TARGET, params=None, out_path=""):
     """Chains of the given samplers for the given replicas (training first when
-    params is None); a JSON-able dict that target_combine merges."""
+    params is None); a JSON-able dict that target_combine merges, also written
+    to out_path after every replica."""
     out = dict(config={k: (list(v) if isinstance(v, tuple) else v) for k, v in cfg.items()}, chains=[])
     if params is None:
         params, rep = target_training(cfg)
@@ -250,6 +257,9 @@ def target_run(replicas, samplers=SAMPLERS, cfg=TARGET, params=None):
             c = q_chain(start, cfg, smp, r, params, best)
             c["therm_seconds"] = therm_s
             out["chains"].append(c)
+        if out_path:
+            with open(out_path, "w") as f:
+                json.dump(out, f)
     return out
 
 
@@ -296,13 +306,26 @@ def target_combine(runs):
                     loo.append(a["eff_Q_per_s"] / b["eff_Q_per_s"])
                 res[smp]["eff_Q_ratio_err"] = jackknife(loo)
     if "plain_fp32" in res and "plain_fp64" in res:
-        # FP64 rate with the pooled tau_int,Q of the plain kernel (FP32 and FP64 chains)
-        pooled = gamma_method_replicas([c["Q"] for s in ("plain_fp32", "plain_fp64") for c in by[s].values()])
+        # The FP64 path with tau_int,Q of its FP32 twin (the same Markov kernel:
+        # the same proposals from the same streams and the same accept rule, only
+        # the rounding differs), which runs long chains at a third of the cost:
+        # effective samples per second = 1 / (2 tau_int,Q [sweeps] x seconds per
+        # sweep, measurements included).  Ratios with a delete-one-replica
+        # jackknife over the replicas all three samplers share.
+        def eff_twin(keep, smp):
+            a = stats([by[smp][r] for r in keep])
+            tw = stats([by["plain_fp32"][r] for r in keep])
+            f = stats([by["plain_fp64"][r] for r in keep])
+            return (1.0 / (2.0 * a["tau_Q"] * a["sweep_seconds"])) / (1.0 / (2.0 * tw["tau_Q"] * f["sweep_seconds"]))
         f64 = res["plain_fp64"]
-        f64["tau_Q_pooled_plain"] = pooled.tau_int * chains[0]["meas_every"]
-        f64["eff_Q_per_s_pooled_tau"] = f64["n_meas"] / (2.0 * pooled.tau_int) / f64["wall_s"]
+        f64["eff_Q_per_s_twin_tau"] = 1.0 / (2.0 * res["plain_fp32"]["tau_Q"] * f64["sweep_seconds"])
         for smp in res:
-            res[smp]["eff_Q_ratio_vs_plain_fp64_pooled_tau"] = res[smp]["eff_Q_per_s"] / f64["eff_Q_per_s_pooled_tau"]
+            res[smp]["eff_Q_ratio_vs_plain_fp64_twin_tau"] = (1.0 / (2.0 * res[smp]["tau_Q"] * res[smp]["sweep_seconds"])
+                                                            / f64["eff_Q_per_s_twin_tau"])
+            shared = sorted(set(by[smp]) & set(by["plain_fp32"]) & set(by["plain_fp64"]))
+            if len(shared) >= 2:
+                loo = [eff_twin([r for r in shared if r != k], smp) for k in shared]
+                res[smp]["eff_Q_ratio_twin_tau_err"] = jackknife(loo)
     return dict(config=runs[0]["config"], best_eps=runs[0].get("best_eps"), samplers=res,
                 training=next((r["training"] for r in runs if r.get("training")), None))
 
@@ -324,7 +347,7 @@ def _main():
     t = sub.add_parser("target", help="effective Q samples/s at 32^3x64, beta=6.2, per sampler")
     t.add_argument("--replicas", default="0,1,2,3")
     t.add_argument("--samplers", default=",".join(SAMPLERS))
-    t.add_argument("--sweeps", type=int, default=TARGET["sweeps"])
+    t.add_argument("--sweeps", type=int, default=0, help="one chain length for all samplers (default: per sampler)")
     t.add_argument("--meas-every", type=int, default=TARGET["meas_every"])
     t.add_argument("--therm", type=int, default=TARGET["therm"])
     t.add_argument("--dims", default="32,32,32,64")
@@ -334,18 +357,16 @@ def _main():
     c.add_argument("files", nargs="+")
     a = ap.parse_args()
     if a.study == "target":
-        cfg = dict(TARGET, sweeps=a.sweeps, meas_every=a.meas_every, therm=a.therm,
-                   dims=tuple(int(x) for x in a.dims.split(",")))
+        cfg = dict(TARGET, meas_every=a.meas_every, therm=a.therm, dims=tuple(int(x) for x in a.dims.split(",")))
+        if a.sweeps:  # one length for every sampler
+            cfg["sweeps"], cfg["sweeps_by"] = a.sweeps, {}
         params = None
         if a.params:
             with open(a.params) as f:
                 prev = json.load(f)
             params = prev["params"]
             cfg["best_eps"] = prev["best_eps"]
-        r = target_run([int(x) for x in a.replicas.split(",")], a.samplers.split(","), cfg, params)
-        if a.out:
-            with open(a.out, "w") as f:
-                json.dump(r, f)
+        r = target_run([int(x) for x in a.replicas.split(",")], a.samplers.split(","), cfg, params, a.out)
         print(json.dumps(target_combine([r])["samplers"]))
         return
     if a.study == "target-combine":

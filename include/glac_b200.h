@@ -149,6 +149,11 @@ glac_status glac_flow_configuration(glac_ctx *ctx, const double *host_links, int
  * n_steps flow steps of the current field (CUDA events on the context's
  * stream); advances the field by n_steps. */
 glac_status glac_flow_stage_times(glac_ctx *ctx, int n_steps, double *seconds3);
+/* The same for flow steps that measure the field before each step inside
+ * stage 0 ("fused_measure" on): seconds4 = [stage 0 with the clover parts,
+ * the measurement's per-site combination and reduction, stage 1, stage 2].
+ * GLAC_ERR_STATE where the measurement is not fused for this context. */
+glac_status glac_flow_stage_times_measured(glac_ctx *ctx, int n_steps, double *seconds4);
 
 /* Launch-variant autotuner (no reference counterpart): times each launch
  * variant (register cap / resident blocks per SM) of the flow-stage,

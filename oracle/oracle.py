@@ -43,7 +43,9 @@ def build(ref: bool = True) -> None:
     """Compile the C restatement, and the reference libraries when its sources exist."""
     targets = ["oracle"]
     if ref and os.path.isdir(REF_SRC):
-        targets += ["ref", "ref-native"]
+        targets += ["ref", "ref-native", "ref-bin"]
+        if os.path.exists(os.path.join(HERE, "..", "glac_b200", "libglac_b200.so")):
+            targets.append("ref-bin-bound")
     subprocess.run(["make", "-s", "-C", HERE, "-j8", f"REF_SRC={REF_SRC}", *targets], check=True)
 
 

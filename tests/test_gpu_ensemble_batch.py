@@ -8,6 +8,8 @@ The CUDA-graph schedule equals the eager one, and replays draw fresh numbers.
 import numpy as np
 import pytest
 
+from conftest import assert_obs_close
+
 pytestmark = pytest.mark.gpu
 
 DIMS = [(4, 4, 4, 8), (6, 4, 4, 4), (8, 8, 8, 16), (4, 6, 8, 10)]
@@ -46,7 +48,9 @@ def test_ensemble_matches_single_contexts(g, ens, prec, tol):
             want_obs = L.flow(4)
         assert rel(links[i], want_links) < tol, i
         assert abs(acc[i] - a) < 1e-12 if prec == "fp64" else abs(acc[i] - a) < 0.01, i
-        assert rel(obs[i], want_obs) < tol * 10, i
+        # the single context measures inside its flow stage 0, the ensemble in a
+        # pass of its own: the same quantities to rounding, quantity by quantity
+        assert_obs_close(obs[i], want_obs, tol * 10, f"lattice {i}")
 
 
 def test_graph_equals_eager_and_replays_draw_fresh_numbers(g, ens):
