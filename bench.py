@@ -587,7 +587,9 @@ def run_profile(args):
         return
     L = g.Lattice(dims, beta=BETA, precision=args.precision, flow_eps=FLOW_EPS, seed=5, device=0)
     L.hot_start(7)
-    L.set_option("fused_measure", int(args.fused))
+    if args.fused >= 0:
+        L.set_option("fused_measure", int(args.fused))
+    L.set_option("fused_combine", int(args.fused_combine))
     if args.tune:
         L.tuning = [int(x) for x in args.tune.split(",")]
     if args.profile == "learned":
@@ -618,7 +620,7 @@ def run_profile(args):
         sec = e0.elapsed_time(e1) / 1e3 / args.time_reps
         stages = L.flow_stage_times(5) if args.profile == "flow" else None
         print(json.dumps({"profile": args.profile, "dims": dims, "precision": args.precision, "tune": L.tuning,
-                          "fused_measure": int(args.fused),
+                          "fused_measure": int(args.fused), "fused_combine": int(args.fused_combine),
                           "ms_per_step": sec * 1e3,
                           "rate": (4 * V if args.profile in ("metropolis", "learned") else V) / sec,
                           "stage_ms": None if stages is None else [x * 1e3 for x in stages]}))
@@ -642,7 +644,10 @@ def main():
     ap.add_argument("--precision", default="fp32")
     ap.add_argument("--no-obs", action="store_true")
     ap.add_argument("--time-reps", type=int, default=0)
-    ap.add_argument("--fused", type=int, default=1, help="profile mode: measurement inside flow stage 0 (1) or a pass of its own (0)")
+    ap.add_argument("--fused", type=int, default=-1,
+                    help="profile mode: measurement inside flow stage 0 (1: uncapped kernel, 2: 128-register kernel) "
+                         "or a pass of its own (0); default: the library's choice per precision")
+    ap.add_argument("--fused-combine", type=int, default=1, help="profile mode: its reduction inside stage 1 (1) or not (0)")
     ap.add_argument("--tune", default="", help="launch variants flow,metropolis,observables (profile mode)")
     args = ap.parse_args()
     if args.profile:

@@ -38,6 +38,7 @@ struct glac_ctx {
     Proposal prop;                // prop.net null: the fixed spread su3_eps
     void *clover = nullptr;       // clover parts of the measurement fused into flow stage 0 (first use)
     int fused_measure = 1;        // measure inside flow stage 0 where the lattice allows it (2: 128-register cap)
+    bool fused_combine = true;    // that measurement's reduction inside stage 1 where the lattice allows it
     bool has_field = false;
     std::string err;
 };
@@ -174,9 +175,21 @@ void flow_step(glac_ctx *c, cudaEvent_t *ev = nullptr, double *meas_out = nullpt
     const double beta[3] = {0.0, -(eps * 0.4722222222222222), -1.0};
     if (ev) ck(cudaEventRecord(ev[0], c->stream), "event");
     int e = 1;
+    // the measurement's per-site combination and reduction: folded into stage 1
+    // where the lattice's half time slices are whole 128-site blocks
+    const bool in_stage1 = meas_out && c->fused_combine && obs_combine_in_stage1(c->g, c->plan);
     for (int stage = 0; stage < 3; stage++) {
         const int src = c->cur, dst = c->cur ^ 1;
-        if (stage == 0 && meas_out) {
+        if (stage == 1 && in_stage1) {
+            if (c->d.precision == GLAC_FP64)
+                launch_flow_stage1_combine(c->g, f64(c, src), f64(c, dst), z64(c), c->d.exp_func, alpha[1], beta[1],
+                                           clover_view<double>(c), c->plan, c->partial, meas_out, c->stream);
+            else
+                launch_flow_stage1_combine(c->g, f32(c, src), f32(c, dst), z32(c), c->d.exp_func, alpha[1], beta[1],
+                                           clover_view<float>(c), c->plan, c->partial, meas_out, c->stream);
+            ck_launch("flow stage 1 with the measurement's reduction");
+            c->launches += 2;
+        } else if (stage == 0 && meas_out) {
             ensure_clover(c);
             const int regs = c->fused_measure == 2 ? 128 : 0;
             if (c->d.precision == GLAC_FP64) {
@@ -185,17 +198,17 @@ void flow_step(glac_ctx *c, cudaEvent_t *ev = nullptr, double *meas_out = nullpt
                                         c->stream);
                 ck_launch("flow stage 0 with measurement");
                 if (ev) ck(cudaEventRecord(ev[e++], c->stream), "event");
-                launch_obs_combine(c->g, cp, c->plan, c->partial, meas_out, c->stream);
+                if (!in_stage1) launch_obs_combine(c->g, cp, c->plan, c->partial, meas_out, c->stream);
             } else {
                 const CloverParts<float> cp = clover_view<float>(c);
                 launch_flow_stage0_meas(c->g, f32(c, src), f32(c, dst), z32(c), cp, c->d.exp_func, alpha[0], regs,
                                         c->stream);
                 ck_launch("flow stage 0 with measurement");
                 if (ev) ck(cudaEventRecord(ev[e++], c->stream), "event");
-                launch_obs_combine(c->g, cp, c->plan, c->partial, meas_out, c->stream);
+                if (!in_stage1) launch_obs_combine(c->g, cp, c->plan, c->partial, meas_out, c->stream);
             }
             ck_launch("measurement from clover parts");
-            c->launches += 3;
+            c->launches += in_stage1 ? 1 : 3;
         } else {
             if (c->d.precision == GLAC_FP64)
                 launch_flow_stage(c->g, f64(c, src), f64(c, dst), z64(c), stage, c->d.exp_func, alpha[stage],
@@ -314,6 +327,14 @@ glac_status glac_set_option(glac_ctx *c, const char *key, long value) {
             return GLAC_ERR_ARG;
         }
         c->fused_measure = (int)value;
+        return GLAC_OK;
+    }
+    if (std::string(key) == "fused_combine") {
+        if (value != 0 && value != 1) {
+            c->err = "fused_combine takes 0 or 1";
+            return GLAC_ERR_ARG;
+        }
+        c->fused_combine = value != 0;
         return GLAC_OK;
     }
     if (std::string(key) == "su2_sign_flips") {

@@ -46,6 +46,9 @@ struct glac_ensemble {
     int obs_steps = -1;  // the layout the slots' obs pointers describe
     double *staging = nullptr;
     size_t staging_cap = 0;
+    void *clover = nullptr;                // clover parts of the measurement inside flow stage 0
+    std::vector<size_t> off_clover;        // bytes
+    bool fused_measure = true;             // measure inside flow stage 0 (all lattices fit the parts' offsets)
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_sweeps = -1, graph_steps = -1;
@@ -120,12 +123,27 @@ size_t obs_offset(const glac_ensemble *E, int i, int rows) {
     return o;
 }
 
+// clover parts of lattice i: 12 slots in the force layout, then 4 plaquette sums per site
+size_t lattice_clover_bytes(int prec, const Geom &g) {
+    return 3 * lattice_force_bytes(prec, g) + 8 * (size_t)g.Vh * (prec == GLAC_FP64 ? sizeof(double) : sizeof(float));
+}
+template <typename T> CloverParts<T> clover_of(glac_ensemble *E, int i) {
+    CloverParts<T> cp;
+    char *base = E->clover ? static_cast<char *>(E->clover) + E->off_clover[i] : nullptr;
+    cp.ah.p = reinterpret_cast<decltype(cp.ah.p)>(base);
+    cp.ah.Vh = E->geo[i].Vh;
+    cp.ah.Vh32 = round32(E->geo[i].Vh);
+    cp.plaq = base ? reinterpret_cast<T *>(base + 3 * lattice_force_bytes(E->d.precision, E->geo[i])) : nullptr;
+    return cp;
+}
+
 template <typename T> void upload_slots(glac_ensemble *E, int rows) {
     std::vector<LatSlot<T>> S(E->M);
     for (int i = 0; i < E->M; i++) {
         S[i].g = E->geo[i];
         for (int r = 0; r < 3; r++) S[i].f[r] = field_of<T>(E, r, i);
         S[i].z = force_of<T>(E, i);
+        S[i].cp = clover_of<T>(E, i);
         S[i].nb = E->plan[i].nb;
         S[i].Bv = E->plan[i].Bv;
         S[i].partial = E->partial + E->off_partial[i];
@@ -189,15 +207,27 @@ template <typename T> void flow_t(glac_ensemble *E, int n, bool measure) {
     const bool fp32 = sizeof(T) == 4;
     const int phase = variant_shape(FAM_FLOW, fp32, E->tune[FAM_FLOW]) == 1 ? ENS_FLOW1 : ENS_FLOW0;
     int cur = 1;
-    if (measure) observe_t<T>(E, cur, 0);
+    // the measurement after step k inside stage 0 of step k + 1 (the field that
+    // stage flows is the one to measure), the last one in a pass of its own
+    const bool fused = measure && E->fused_measure && E->clover;
+    if (measure && (!fused || n == 0)) observe_t<T>(E, cur, 0);
     for (int step = 0; step < n; step++) {
         for (int stage = 0; stage < 3; stage++) {
-            launch_ens_flow_stage<T>(slots_of<T>(E), E->start[phase], E->nblk[phase], E->M, cur, 3 - cur, stage,
-                                     alpha[stage], bet[stage], E->tune[FAM_FLOW], E->stream);
-            E->launches++;
+            if (stage == 0 && fused) {
+                // FP32: the 128-register kernel, FP64: the compiler's own allocation
+                launch_ens_flow_stage0_meas<T>(slots_of<T>(E), E->start[ENS_FLOW0], E->nblk[ENS_FLOW0], E->M, cur,
+                                               3 - cur, alpha[0], sizeof(T) == 4 ? 128 : 0, E->stream);
+                launch_ens_obs_combine<T>(slots_of<T>(E), E->start[ENS_OBS], E->nblk[ENS_OBS], E->M, step,
+                                          E->stream);
+                E->launches += 3;
+            } else {
+                launch_ens_flow_stage<T>(slots_of<T>(E), E->start[phase], E->nblk[phase], E->M, cur, 3 - cur, stage,
+                                         alpha[stage], bet[stage], E->tune[FAM_FLOW], E->stream);
+                E->launches++;
+            }
             cur = 3 - cur;
         }
-        if (measure) observe_t<T>(E, cur, step + 1);
+        if (measure && (!fused || step == n - 1)) observe_t<T>(E, cur, step + 1);
     }
 }
 
@@ -309,7 +339,7 @@ glac_status glac_ensemble_create(int n, const int *dims, const double *betas, co
     E->d = *common;
     E->M = n;
     glac_status s = eguarded(E, [&] {
-        size_t fo = 0, zo = 0, po = 0;
+        size_t fo = 0, zo = 0, po = 0, co = 0;
         std::vector<int> st[ENS_NPHASE];
         for (int k = 0; k < ENS_NPHASE; k++) st[k].push_back(0);
         for (int i = 0; i < n; i++) {
@@ -321,6 +351,9 @@ glac_status glac_ensemble_create(int n, const int *dims, const double *betas, co
             E->off_field.push_back(fo);
             E->off_force.push_back(zo);
             E->off_partial.push_back(po);
+            E->off_clover.push_back(co);
+            co += align256(lattice_clover_bytes(E->d.precision, g));
+            if (!clover_offsets_fit(g.V, E->d.precision == GLAC_FP64)) E->fused_measure = false;
             fo += align256(lattice_field_bytes(E->d.precision, g));
             zo += align256(lattice_force_bytes(E->d.precision, g));
             po += 3 * (size_t)pl.nblocks;
@@ -333,6 +366,7 @@ glac_status glac_ensemble_create(int n, const int *dims, const double *betas, co
         for (int r = 0; r < 3; r++) eck(cudaMalloc(&E->field[r], fo), "field alloc");
         eck(cudaMalloc(&E->force, zo), "force alloc");
         eck(cudaMalloc(&E->partial, po * sizeof(double)), "partial alloc");
+        if (E->fused_measure) eck(cudaMalloc(&E->clover, co), "clover parts alloc");
         const size_t slot_bytes = E->d.precision == GLAC_FP64 ? sizeof(LatSlot<double>) : sizeof(LatSlot<float>);
         eck(cudaMalloc(&E->slots, n * slot_bytes), "slots alloc");
         eck(cudaMalloc(&E->acc, n * sizeof(unsigned long long)), "acc alloc");
@@ -363,7 +397,7 @@ void glac_ensemble_destroy(glac_ensemble *E) {
     if (E->stream) cudaStreamSynchronize(E->stream);
     drop_graph(E);
     for (void *p : {E->field[0], E->field[1], E->field[2], E->force, (void *)E->partial, E->slots, (void *)E->acc,
-                    (void *)E->sweep_dev, (void *)E->obs, (void *)E->staging})
+                    (void *)E->sweep_dev, (void *)E->obs, (void *)E->staging, E->clover})
         if (p) cudaFree(p);
     for (int k = 0; k < ENS_NPHASE; k++)
         if (E->start[k]) cudaFree(E->start[k]);
@@ -379,6 +413,15 @@ glac_status glac_ensemble_set_option(glac_ensemble *E, const char *key, long val
     if (!E || !key) return GLAC_ERR_ARG;
     if (std::string(key) == "su2_sign_flips" && (value == 0 || value == 1)) {
         E->flips = value != 0;
+        drop_graph(E);
+        return GLAC_OK;
+    }
+    if (std::string(key) == "fused_measure" && (value == 0 || value == 1)) {
+        if (value == 1 && !E->clover) {
+            E->err = "fused_measure: a lattice of this ensemble is too large for the clover parts' 32-bit offsets";
+            return GLAC_ERR_ARG;
+        }
+        E->fused_measure = value != 0;
         drop_graph(E);
         return GLAC_OK;
     }

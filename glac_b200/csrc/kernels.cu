@@ -920,6 +920,20 @@ void launch_observables(const Geom &g, const LinkField<T> &L, const ObsPlan &pla
 // direction sums; Q(t), E and the plaquette reduced as in observables_body (same
 // blocks, same fixed order), then k_obs_finalize.
 template <typename T>
+__device__ __forceinline__ void combine_site(const Geom &g, const CloverParts<T> &cp, int p, int s, double &plaq,
+                                             double &en, double &qt) {
+    AH8<T> F[6];
+#pragma unroll
+    for (int pl = 0; pl < 6; pl++) F[pl] = ah_add(cp.ah.load(2 * pl, p, s), cp.ah.load(2 * pl + 1, p, s));
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) plaq += (double)cp.plaq[(mu * 2 + p) * g.Vh + s];
+    // q = -[ReTr(F_01 F_23) + ReTr(F_02 F_31) + ReTr(F_03 F_12)], F_31 = -F_13
+    qt = -((double)retr_ah(F[0], F[5]) - (double)retr_ah(F[1], F[4]) + (double)retr_ah(F[2], F[3]));
+#pragma unroll
+    for (int pl = 0; pl < 6; pl++) en += (double)retr_ah(F[pl], F[pl]);
+}
+
+template <typename T>
 __global__ void __launch_bounds__(256) k_obs_combine(Geom g, CloverParts<T> cp, int nb, int Bv, double *partial) {
     const int b = blockIdx.x;
     const int t = b / (2 * nb);
@@ -929,19 +943,66 @@ __global__ void __launch_bounds__(256) k_obs_combine(Geom g, CloverParts<T> cp, 
     const bool valid = (int)threadIdx.x < Bv;
     const int s = t * half_slice + j * Bv + (valid ? (int)threadIdx.x : 0);
     double plaq = 0.0, en = 0.0, qt = 0.0;
-    if (valid) {
-        AH8<T> F[6];
-#pragma unroll
-        for (int pl = 0; pl < 6; pl++) F[pl] = ah_add(cp.ah.load(2 * pl, p, s), cp.ah.load(2 * pl + 1, p, s));
-#pragma unroll
-        for (int mu = 0; mu < 4; mu++) plaq += (double)cp.plaq[(mu * 2 + p) * g.Vh + s];
-        // q = -[ReTr(F_01 F_23) + ReTr(F_02 F_31) + ReTr(F_03 F_12)], F_31 = -F_13
-        qt = -((double)retr_ah(F[0], F[5]) - (double)retr_ah(F[1], F[4]) + (double)retr_ah(F[2], F[3]));
-#pragma unroll
-        for (int pl = 0; pl < 6; pl++) en += (double)retr_ah(F[pl], F[pl]);
-    }
+    if (valid) combine_site(g, cp, p, s, plaq, en, qt);
     obs_block_reduce(plaq, en, qt, partial, b);
 }
+
+// Flow stage 1 that also does the measurement's per-site combination and
+// block reduction: the blocks of the mu = 0 planes (shape 0: 128 consecutive
+// sites of one parity) combine the clover parts of their own 128 sites after
+// their links' stage-1 update.  For lattices whose half time slice is a
+// multiple of 128 sites, so that each such block lies in one (t, parity) half
+// slice and its partial sums sit where the observable plan's 128-site blocks
+// put them (obs_combine_in_stage1).  Launch bounds keep the plain stage's
+// occupancy: five blocks of 128 per SM in FP32 (96 registers), three in FP64.
+template <typename T, int KIND>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 3) k_flow_stage1_combine(Geom g, LinkField<T> in, LinkField<T> out,
+                                                             ForceField<T> zf, T alpha, T beta, CloverParts<T> cp,
+                                                             double *partial) {
+    flow_stage_body<T, KIND, 1, 0>(g, in, out, zf, alpha, beta, blockIdx.x);
+    const int plane = blockIdx.x & 7;
+    if (plane >= 2) return;  // a whole block returns together
+    const int p = plane & 1;
+    const int s0 = (blockIdx.x >> 3) * 128, s = s0 + threadIdx.x;
+    const int half_slice = g.Vh / g.N[3];
+    const int nb = half_slice >> 7;
+    const int t = s0 / half_slice, j = (s0 - t * half_slice) >> 7;
+    double plaq = 0.0, en = 0.0, qt = 0.0;
+    combine_site(g, cp, p, s, plaq, en, qt);
+    obs_block_reduce(plaq, en, qt, partial, (t * 2 + p) * nb + j);
+}
+
+bool obs_combine_in_stage1(const Geom &g, const ObsPlan &plan) {
+    const int half_slice = g.Vh / g.N[3];
+    return half_slice % 128 == 0 && plan.Bv == 128 && plan.nb == half_slice / 128;
+}
+
+template <typename T>
+void launch_flow_stage1_combine(const Geom &g, const LinkField<T> &in, const LinkField<T> &out,
+                                const ForceField<T> &zf, int kind, double alpha, double beta,
+                                const CloverParts<T> &cp, const ObsPlan &plan, double *partial, double *obs_out,
+                                cudaStream_t st) {
+    if (g.N[3] > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
+    if (!obs_combine_in_stage1(g, plan)) throw std::invalid_argument("lattice does not allow the stage-1 combine");
+    const dim3 grid(8 * (g.Vh / 128));
+    const T a = (T)alpha, b = (T)beta;
+    switch (kind) {
+    case 0: k_flow_stage1_combine<T, 0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, cp, partial); break;
+    case 1: k_flow_stage1_combine<T, 1><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, cp, partial); break;
+    case 2: k_flow_stage1_combine<T, 2><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, cp, partial); break;
+    case 3: k_flow_stage1_combine<T, 3><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, cp, partial); break;
+    default: throw std::invalid_argument("bad exp kind");
+    }
+    k_obs_finalize<<<1, 1024, 0, st>>>(g.N[3], plan.nb, g.V, partial, obs_out);
+}
+template void launch_flow_stage1_combine<double>(const Geom &, const LinkField<double> &, const LinkField<double> &,
+                                                 const ForceField<double> &, int, double, double,
+                                                 const CloverParts<double> &, const ObsPlan &, double *, double *,
+                                                 cudaStream_t);
+template void launch_flow_stage1_combine<float>(const Geom &, const LinkField<float> &, const LinkField<float> &,
+                                                const ForceField<float> &, int, double, double,
+                                                const CloverParts<float> &, const ObsPlan &, double *, double *,
+                                                cudaStream_t);
 
 template <typename T>
 void launch_obs_combine(const Geom &g, const CloverParts<T> &cp, const ObsPlan &plan, double *partial, double *out,
@@ -1614,6 +1675,48 @@ void launch_ens_observables(const LatSlot<T> *slots, const int *start, int nbloc
     kb_obs_finalize<T><<<M, 1024, 0, st>>>(slots, meas);
 }
 
+#define GLAC_ENS_MEAS_KERNEL(NAME, ATTR)                                                                     \
+    template <typename T>                                                                                  \
+    __global__ void ATTR NAME(const LatSlot<T> *__restrict__ slots, const int *__restrict__ start, int M,    \
+                              int src, int dst, T alpha) {                                                 \
+        const int i = slot_of(start, M, blockIdx.x);                                                       \
+        const LatSlot<T> &S = slots[i];                                                                    \
+        flow_stage0_meas_body<T, EXP_MORNINGSTAR>(S.g, S.f[src], S.f[dst], S.z, S.cp, alpha,                \
+                                                  blockIdx.x - __ldg(start + i));                          \
+    }
+GLAC_ENS_MEAS_KERNEL(kb_flow_stage0_meas, __launch_bounds__(128))
+GLAC_ENS_MEAS_KERNEL(kb_flow_stage0_meas_r128, __maxnreg__(128))
+#undef GLAC_ENS_MEAS_KERNEL
+
+template <typename T>
+void launch_ens_flow_stage0_meas(const LatSlot<T> *slots, const int *start, int nblocks, int M, int src, int dst,
+                                 double alpha, int regs, cudaStream_t st) {
+    if (regs == 128) kb_flow_stage0_meas_r128<T><<<nblocks, 128, 0, st>>>(slots, start, M, src, dst, (T)alpha);
+    else kb_flow_stage0_meas<T><<<nblocks, 128, 0, st>>>(slots, start, M, src, dst, (T)alpha);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) kb_obs_combine(const LatSlot<T> *__restrict__ slots,
+                                                      const int *__restrict__ start, int M) {
+    const int i = slot_of(start, M, blockIdx.x);
+    const LatSlot<T> &S = slots[i];
+    const int b = blockIdx.x - __ldg(start + i);
+    const int nb = S.nb, Bv = S.Bv;
+    const int t = b / (2 * nb), p = (b / nb) & 1, j = b % nb;
+    const int half_slice = S.g.Vh / S.g.N[3];
+    const bool valid = (int)threadIdx.x < Bv;
+    const int s = t * half_slice + j * Bv + (valid ? (int)threadIdx.x : 0);
+    double plaq = 0.0, en = 0.0, qt = 0.0;
+    if (valid) combine_site(S.g, S.cp, p, s, plaq, en, qt);
+    obs_block_reduce(plaq, en, qt, S.partial, b);
+}
+template <typename T>
+void launch_ens_obs_combine(const LatSlot<T> *slots, const int *start, int nblocks, int M, int meas,
+                            cudaStream_t st) {
+    kb_obs_combine<T><<<nblocks, 128, 0, st>>>(slots, start, M);
+    kb_obs_finalize<T><<<M, 1024, 0, st>>>(slots, meas);
+}
+
 __global__ void k_advance(uint32_t *counter, uint32_t by) { counter[0] += by; }
 void launch_advance(uint32_t *counter, uint32_t by, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(counter, by); }
 
@@ -1624,7 +1727,10 @@ void launch_advance(uint32_t *counter, uint32_t by, cudaStream_t st) { k_advance
     template void launch_ens_flow_stage<T>(const LatSlot<T> *, const int *, int, int, int, int, int, double,  \
                                            double, int, cudaStream_t);                                        \
     template void launch_ens_observables<T>(const LatSlot<T> *, const int *, int, int, int, int, int,         \
-                                            cudaStream_t);
+                                            cudaStream_t);                                                    \
+    template void launch_ens_flow_stage0_meas<T>(const LatSlot<T> *, const int *, int, int, int, int, double, \
+                                                 int, cudaStream_t);                                          \
+    template void launch_ens_obs_combine<T>(const LatSlot<T> *, const int *, int, int, int, cudaStream_t);
 GLAC_ENS_INST(double)
 GLAC_ENS_INST(float)
 #undef GLAC_ENS_INST

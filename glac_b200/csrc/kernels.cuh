@@ -86,6 +86,14 @@ void launch_flow_stage0_meas(const Geom &g, const LinkField<T> &in, const LinkFi
 template <typename T>
 void launch_obs_combine(const Geom &g, const CloverParts<T> &cp, const ObsPlan &plan, double *partial, double *out,
                         cudaStream_t st);
+// Flow stage 1 with the measurement's combination and reduction folded in
+// (where obs_combine_in_stage1 holds), then the final reduction into obs_out.
+bool obs_combine_in_stage1(const Geom &g, const ObsPlan &plan);
+template <typename T>
+void launch_flow_stage1_combine(const Geom &g, const LinkField<T> &in, const LinkField<T> &out,
+                                const ForceField<T> &zf, int kind, double alpha, double beta,
+                                const CloverParts<T> &cp, const ObsPlan &plan, double *partial, double *obs_out,
+                                cudaStream_t st);
 // whether the 12 clover-part slots of a lattice fit 32-bit element offsets
 inline bool clover_offsets_fit(long long V, bool fp64) {
     const long long vh32 = ((V / 2) + 31) / 32 * 32;
@@ -156,6 +164,7 @@ template <typename T> struct LatSlot {
     int nb, Bv;               // observable plan (blocks of <= 128 threads)
     double *partial;          // 3 doubles per observable block
     double *obs;              // this lattice's measurement rows (3 + Nt each)
+    CloverParts<T> cp;        // clover parts of the measurement inside flow stage 0 (cp.ah.p null: none)
     unsigned long long *acc;  // accepted proposals
     float beta;
     uint32_t stream;          // Philox stream
@@ -177,6 +186,15 @@ void launch_ens_flow_stage(const LatSlot<T> *slots, const int *start, int nblock
 template <typename T>
 void launch_ens_observables(const LatSlot<T> *slots, const int *start, int nblocks, int M, int fsel,
                             int meas, int variant, cudaStream_t st);
+// Flow stage 0 of every lattice with its measurement's clover parts (block
+// table of the shape-0 flow phase), and the measurement from those parts into
+// measurement row `meas` (block table of the observable phase).
+template <typename T>
+void launch_ens_flow_stage0_meas(const LatSlot<T> *slots, const int *start, int nblocks, int M, int src, int dst,
+                                 double alpha, int regs, cudaStream_t st);
+template <typename T>
+void launch_ens_obs_combine(const LatSlot<T> *slots, const int *start, int nblocks, int M, int meas,
+                            cudaStream_t st);
 void launch_advance(uint32_t *counter, uint32_t by, cudaStream_t st);
 
 }  // namespace glac

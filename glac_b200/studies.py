@@ -312,18 +312,22 @@ def target_combine(runs):
         # effective samples per second = 1 / (2 tau_int,Q [sweeps] x seconds per
         # sweep, measurements included).  Ratios with a delete-one-replica
         # jackknife over the replicas all three samplers share.
+        # (The FP64 seconds per sweep come from all its chains: a timing, not a
+        # statistical estimate; the jackknife runs over the replicas that the
+        # sampler and the FP32 twin share.)
+        f64 = res["plain_fp64"]
+
         def eff_twin(keep, smp):
             a = stats([by[smp][r] for r in keep])
             tw = stats([by["plain_fp32"][r] for r in keep])
-            f = stats([by["plain_fp64"][r] for r in keep])
-            return (1.0 / (2.0 * a["tau_Q"] * a["sweep_seconds"])) / (1.0 / (2.0 * tw["tau_Q"] * f["sweep_seconds"]))
-        f64 = res["plain_fp64"]
+            return (tw["tau_Q"] * f64["sweep_seconds"]) / (a["tau_Q"] * a["sweep_seconds"])
+
         f64["eff_Q_per_s_twin_tau"] = 1.0 / (2.0 * res["plain_fp32"]["tau_Q"] * f64["sweep_seconds"])
         for smp in res:
             res[smp]["eff_Q_ratio_vs_plain_fp64_twin_tau"] = (1.0 / (2.0 * res[smp]["tau_Q"] * res[smp]["sweep_seconds"])
                                                             / f64["eff_Q_per_s_twin_tau"])
-            shared = sorted(set(by[smp]) & set(by["plain_fp32"]) & set(by["plain_fp64"]))
-            if len(shared) >= 2:
+            shared = sorted(set(by[smp]) & set(by["plain_fp32"]))
+            if len(shared) >= 2 and smp != "plain_fp64":
                 loo = [eff_twin([r for r in shared if r != k], smp) for k in shared]
                 res[smp]["eff_Q_ratio_twin_tau_err"] = jackknife(loo)
     return dict(config=runs[0]["config"], best_eps=runs[0].get("best_eps"), samplers=res,

@@ -87,7 +87,12 @@ uint64_t glac_launch_count(const glac_ctx *ctx);
  *   per plane instead of the ten of a separate clover pass), and the last one
  *   in a pass of its own; 1 uses the stage kernel's own register allocation, 2
  *   a 128-register variant; 0 measures every field in a pass of its own.  The
- *   results are the same to rounding. */
+ *   results are the same to rounding.
+ *   "fused_combine" (default 1): with fused_measure on, the measurement's
+ *   per-site combination and block reduction run inside the step's second
+ *   stage where each half time slice is a whole number of 128-site blocks
+ *   (Nx Ny Nz / 2 divisible by 128), else in a pass of their own; 0: always a
+ *   pass of their own. */
 glac_status glac_set_option(glac_ctx *ctx, const char *key, long value);
 
 /* ---- field --------------------------------------------------------------- */
@@ -301,7 +306,9 @@ const char *glac_ensemble_last_error(const glac_ensemble *ens);
 /* Message of the last failed glac_ensemble_create on this thread. */
 const char *glac_ensemble_global_error(void);
 uint64_t glac_ensemble_launch_count(const glac_ensemble *ens);
-/* "su2_sign_flips" 0/1 as for glac_set_option. */
+/* "su2_sign_flips" 0/1 as for glac_set_option; "fused_measure" 1 (default):
+ * each flow measurement inside the next step's first stage, 0: every
+ * measurement in a pass of its own (as glac_set_option). */
 glac_status glac_ensemble_set_option(glac_ensemble *ens, const char *key, long value);
 /* Seeded Haar start of every lattice (as glac_hot_start with the lattice's stream). */
 glac_status glac_ensemble_hot_start(glac_ensemble *ens, uint64_t seed);

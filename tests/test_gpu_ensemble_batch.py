@@ -120,3 +120,18 @@ def test_ensemble_errors(g, ens):
             E.get_links(3)
         with pytest.raises(g.GlacError):
             E.tuning = [0, 0, 5]
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+def test_ensemble_measurement_inside_stage0_matches_standalone(g, ens, prec, tol):
+    # every flow measurement but the last comes from the next step's stage 0;
+    # with fused_measure = 0 each is a pass of its own: the same to rounding
+    kw = dict(precision=prec, seed=SEED, flow_eps=0.02)
+    with ens.Ensemble(DIMS, BETAS, **kw) as A, ens.Ensemble(DIMS, BETAS, **kw) as B:
+        B.set_option("fused_measure", 0)
+        for E in (A, B):
+            E.hot_start(8)
+            E.metropolis(20)
+        oa, ob = A.flow(4), B.flow(4)
+        for i in range(len(DIMS)):
+            assert_obs_close(oa[i], ob[i], 4 * tol, f"lattice {i}")
