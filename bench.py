@@ -51,13 +51,28 @@ STAGE_BYTES_FP64 = tuple(2 * b for b in STAGE_BYTES_FP32)
 NCU_TRAFFIC_STAGE0_FP32 = 636109568 + 837838592  # bytes, one ncu capture of the launch (uncapped variant)
 # stage 0 with the measurement's clover parts: + 12 slots x 32 B + 4 plaquette floats per site written
 STAGE0_MEAS_BYTES_FP32 = STAGE_BYTES_FP32[0] + 12 * 32 + 4 * 4
-NCU_TRAFFIC_STAGE0_MEAS_FP32 = None  # bytes per launch from an ncu capture at 32^3x64 (profiles/)
-FLOPS_PER_SITE_STAGE0_MEAS_FP32 = None  # from ncu instruction counts of that launch (profiles/)
+# dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of that launch at
+# 32^3x64 (k_flow_stage0_meas_r128, profiles/flow_stage0_meas_fp32_32x32x32x64.md)
+NCU_TRAFFIC_STAGE0_MEAS_FP32 = 707364864 + 1667783168
+# FP32 FLOP per site of that launch: (2 x FFMA + FADD + FMUL) thread instructions
+# counted by ncu = (2 x 14,914,945,024 + 1,472,200,704 + 1,400,897,536) / 2,097,152
+FLOPS_PER_SITE_STAGE0_MEAS_FP32 = 15594
 # FP32 floating-point operations per site of one stage-0 launch: 4 links x
 # (2 x FFMA + FADD + FMUL) thread instructions counted by ncu
 # (sm__sass_thread_inst_executed_op_{ffma,fadd,fmul}_pred_on) on the 32^3x64 launch
 FLOPS_PER_SITE_STAGE0_FP32 = 4 * (2 * 1547 + 59 + 95)
 SM_COUNT, FP32_LANES_PER_SM = 148, 128
+# The metric's third leg, effective Q samples/s of the learned FP32 sampler
+# against the plain FP64 GPU path at 32^3x64, beta = 6.2: a study of
+# 4 replicas x tens of thousands of sweeps per sampler (about 40 GPU-minutes),
+# recorded in profiles/eff_q_study_32x32x32x64_b6.2.md and reproduced by
+# `python -m glac_b200.studies target`; bench.py reports it, it does not
+# re-measure it.
+EFF_Q_STUDY = {"measured_in_this_run": False, "source": "profiles/eff_q_study_32x32x32x64_b6.2.md",
+               "ratio_learned_fp32_vs_plain_fp64": 6.94, "err": 0.38,
+               "ratio_ablation_fp32_vs_plain_fp64": 7.25, "ablation_err": 0.37,
+               "estimator": "Q diffusion over 500 sweeps per second of sweeps + measurements, replica jackknife",
+               "plaquette_learned_minus_fp64_sigma": -0.8}
 # Metropolis: algorithmic bytes per link update in FP32 (9 link transfers x 72 B)
 METRO_BYTES_FP32 = 9 * 72
 
@@ -499,6 +514,7 @@ def run_gpu(args):
                                              frac=round(metro_roofline["achieved"] / hbm_peak, 4)),
             "metropolis_link_updates_per_s_fp64": metro64_rate,
             "learned": learned_extra,
+            "eff_Q_samples_study": EFF_Q_STUDY,
             "ensemble_64_uneven": ens_extra,
             "metropolis_acceptance": acc_holder.get("a"),
             "plaq_after_flow": float(obs_last[0]),

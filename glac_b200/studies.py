@@ -330,6 +330,34 @@ def target_combine(runs):
             if len(shared) >= 2 and smp != "plain_fp64":
                 loo = [eff_twin([r for r in shared if r != k], smp) for k in shared]
                 res[smp]["eff_Q_ratio_twin_tau_err"] = jackknife(loo)
+    # Q diffusion: D(lag) = <(Q_{i+lag} - Q_i)^2> over all chains of a sampler.
+    # For lags well below tau_int,Q it grows as 2 <Q^2> lag / tau, so D per
+    # sweep is proportional to the rate at which Q decorrelates, and
+    # D(lag) / (lag x seconds per sweep) compares effective Q samples per second
+    # between samplers without an estimate of tau_int itself, with far smaller
+    # statistical errors when the chains are only tens of tau_int long.
+    meas_every = chains[0]["meas_every"]
+    for lag_sweeps in (200, 500, 1000):
+        k = lag_sweeps // meas_every
+        key = f"Q_diffusion_{lag_sweeps}"
+        for smp, reps in by.items():
+            per = {r: float(np.mean((np.asarray(c["Q"])[k:] - np.asarray(c["Q"])[:-k]) ** 2)) for r, c in reps.items()}
+            n = {r: len(c["Q"]) - k for r, c in reps.items()}
+            D = sum(per[r] * n[r] for r in per) / sum(n.values())
+            res[smp][key] = D
+            if len(per) >= 2:
+                loo = [sum(per[r] * n[r] for r in per if r != q) / sum(n[r] for r in per if r != q) for q in per]
+                res[smp][key + "_err"] = jackknife(loo)
+        if "plain_fp64" in res:
+            base = res["plain_fp64"][key] / res["plain_fp64"]["sweep_seconds"]
+            rel_base = res["plain_fp64"].get(key + "_err", 0.0) / res["plain_fp64"][key]
+            for smp in res:
+                ratio = res[smp][key] / res[smp]["sweep_seconds"] / base
+                res[smp][f"eff_Q_ratio_vs_plain_fp64_diffusion_{lag_sweeps}"] = ratio
+                if smp != "plain_fp64" and key + "_err" in res[smp]:
+                    rel = res[smp][key + "_err"] / res[smp][key]
+                    res[smp][f"eff_Q_ratio_vs_plain_fp64_diffusion_{lag_sweeps}_err"] = ratio * float(
+                        np.hypot(rel, rel_base))
     return dict(config=runs[0]["config"], best_eps=runs[0].get("best_eps"), samplers=res,
                 training=next((r["training"] for r in runs if r.get("training")), None))
 

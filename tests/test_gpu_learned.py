@@ -215,7 +215,14 @@ def test_learned_chain_keeps_reference_plaquette(g):
     assert abs(mean - ref["plaquette"]) < 3 * sigma, (mean, err, ref["plaquette"])
 
 
-def test_trained_spread_beats_fixed_spread(g, torch, learned):
+def test_trained_spread_against_the_method_without_it(g, torch, learned):
+    # What the network gains, on held-out rows (mean squared jump per link
+    # update): over the method without it -- the plain sampler, the reference's
+    # proposal at SU3Eps = 0.24 -- a factor of ~3.3 (3.34 at 32^3 x 64, beta = 6.2);
+    # over the same family at 0.24 ~1.1; against the best fixed spread of the
+    # family, found by a grid search, it ties (0.9999): the network finds that
+    # spread itself and learns almost no per-link variation, so a tie is what
+    # this asserts there.
     grid = learned.DEFAULT_GRID
     with g.Lattice((8, 8, 8, 16), beta=6.0, precision="fp32", seed=3) as L:
         L.hot_start(3)
@@ -223,8 +230,11 @@ def test_trained_spread_beats_fixed_spread(g, torch, learned):
         feat, esj, plain = learned.collect_esj(L, 200, 10, 2, grid, trials=4)
     net, rep = learned.train_proposal(feat, esj, grid, steps=800, batch=4096, lr=3e-3, seed=1, esj_plain=plain)
     net.close()
-    # held-out rows: mean squared jump per link update of the trained network
-    # against the reference's proposal (eps = 0.24) and the family's fixed spreads
-    assert rep["gain_vs_plain"] > 1.5, rep
+    print("learned spread on held-out rows:", {k: rep[k] for k in ("gain_vs_plain", "gain_vs_024",
+                                                                   "gain_vs_best_fixed", "eps_learned_mean",
+                                                                   "eps_learned_std", "best_fixed_eps")})
+    assert rep["gain_vs_plain"] > 2.5, rep
     assert rep["gain_vs_024"] > 1.05, rep
-    assert rep["gain_vs_best_fixed"] > 0.99, rep
+    assert abs(rep["gain_vs_best_fixed"] - 1.0) < 0.01, rep
+    # and its spread lies within one grid step (a factor 1.255) of the best grid point
+    assert abs(np.log(rep["eps_learned_mean"] / rep["best_fixed_eps"])) < np.log(grid[1] / grid[0]), rep
