@@ -181,17 +181,21 @@ void flow_step(glac_ctx *c, cudaEvent_t *ev = nullptr, double *meas_out = nullpt
     for (int stage = 0; stage < 3; stage++) {
         const int src = c->cur, dst = c->cur ^ 1;
         if (stage == 1 && in_stage1) {
+            // the site-per-thread stage where the flow family's chosen variant has that shape
+            const bool site = variant_shape(FAM_FLOW, c->d.precision == GLAC_FP32, c->tune[FAM_FLOW]) == 3;
             if (c->d.precision == GLAC_FP64)
                 launch_flow_stage1_combine(c->g, f64(c, src), f64(c, dst), z64(c), c->d.exp_func, alpha[1], beta[1],
-                                           clover_view<double>(c), c->plan, c->partial, meas_out, c->stream);
+                                           clover_view<double>(c), c->plan, c->partial, meas_out, false, c->stream);
             else
                 launch_flow_stage1_combine(c->g, f32(c, src), f32(c, dst), z32(c), c->d.exp_func, alpha[1], beta[1],
-                                           clover_view<float>(c), c->plan, c->partial, meas_out, c->stream);
+                                           clover_view<float>(c), c->plan, c->partial, meas_out, site, c->stream);
             ck_launch("flow stage 1 with the measurement's reduction");
             c->launches += 2;
         } else if (stage == 0 && meas_out) {
             ensure_clover(c);
-            const int regs = c->fused_measure == 2 ? 128 : 0;
+            // 1: link per thread, compiler's registers; 2: the same capped at 128;
+            // 3 (FP32): site per thread, upper staple products shared
+            const int regs = c->fused_measure == 2 ? 128 : (c->fused_measure == 3 ? 3 : 0);
             if (c->d.precision == GLAC_FP64) {
                 const CloverParts<double> cp = clover_view<double>(c);
                 launch_flow_stage0_meas(c->g, f64(c, src), f64(c, dst), z64(c), cp, c->d.exp_func, alpha[0], regs,
@@ -322,8 +326,9 @@ glac_status glac_sync(glac_ctx *c) {
 glac_status glac_set_option(glac_ctx *c, const char *key, long value) {
     if (!c || !key) return GLAC_ERR_ARG;
     if (std::string(key) == "fused_measure") {
-        if (value < 0 || value > 2) {
-            c->err = "fused_measure takes 0 (off), 1 (on) or 2 (on, 128-register kernel)";
+        if (value < 0 || value > 3 || (value == 3 && c->d.precision != GLAC_FP32)) {
+            c->err = "fused_measure takes 0 (off), 1 (on), 2 (on, 128-register kernel) or, in FP32, 3 (on, a "
+                     "thread per site)";
             return GLAC_ERR_ARG;
         }
         c->fused_measure = (int)value;

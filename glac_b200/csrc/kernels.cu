@@ -27,6 +27,9 @@ namespace glac {
 //   shape 1: a block = the same 16 sites in all 8 planes (half-warp per plane),
 //            so the neighbour links shared by the 8 link directions of a site
 //            are re-read from L1.
+//   shape 3: FP32, a thread per site doing its four links in turn, the upper
+//            staple product of each plane shared between its two links
+//            (flow_stage_site_body below);
 //   shape 2: as shape 0, with the 128-site chunks taken in 4 x 4 tiles of
 //            (z, t) (tiled_chunk), so that a link's neighbours in t are
 //            mostly read while it is still in L2.  An FP64 variant: its
@@ -81,6 +84,141 @@ __device__ __forceinline__ void flow_stage_body(const Geom &g, const LinkField<T
     }
 }
 
+// Shape 3 (FP32): one thread per site, its four links in turn.  The upper
+// staple product of a plane, T_munu = U_nu(n+mu) U_mu(n+nu)^+ (mu < nu), serves
+// both links of the plane at the site: link mu adds T U_nu(n)^+ and keeps T in
+// the thread's shared-memory slot, link nu later adds T^+ U_mu(n)^+ (the same
+// three links) without loading U_nu(n+mu) and U_mu(n+nu) again.  46 SU(3)
+// products per site instead of 52 and 64 link loads instead of 76.  Four slots
+// per thread suffice in the order mu = 0..3 (T_01 -> 0, T_02 -> 1, T_03 -> 2,
+// then T_12 -> 0 and T_13 -> 3 once T_01 is used, T_23 -> 1 once T_02 is).
+// Each thread touches only its own slots, laid out slot-major with the thread
+// index fastest (no bank conflicts, no barrier).
+__host__ __device__ constexpr int tslot(int a, int b) {
+    return a == 0 ? b - 1 : (a == 1 ? (b == 2 ? 0 : 3) : 1);
+}
+constexpr int kSiteBlock = 128;
+
+// MEAS (stage 0 only): also the measurement's clover parts of the planes each
+// link direction takes, as flow_stage0_meas_body does (defined further down).
+__device__ __forceinline__ bool meas_takes(int mu, int nu);
+__host__ __device__ constexpr int plane_of(int a, int b);
+template <typename T> __device__ __forceinline__ AH8<T> proj_ah8(const M3<T> &C);
+template <typename T> __device__ __forceinline__ AH8<T> ah_neg_if(const AH8<T> &F, bool neg);
+
+template <typename T, int KIND, int STAGE, bool MEAS = false>
+__device__ __forceinline__ void flow_stage_site_body(const Geom &g, const LinkField<T> &in, const LinkField<T> &out,
+                                                     const ForceField<T> &zf, T alpha, T beta, int bx, T *slots,
+                                                     const CloverParts<T> *cp = nullptr) {
+    const int p = bx & 1;
+    const int s = (bx >> 1) * kSiteBlock + threadIdx.x;
+    if (s >= g.Vh) return;
+    const int q = p ^ 1;
+    const Site n = site_from_ps(g, p, s);
+    T *my = slots + threadIdx.x;  // element e of slot k at my[(18 k + e) * kSiteBlock]
+#pragma unroll 1
+    for (int mu = 0; mu < 4; mu++) {
+        M3<T> A;
+        set_zero(A);
+        T plaq = T(0);
+        const int f_mu = step_offset(g, n, mu, +1);
+        const int s_mu = (n.lex + f_mu) >> 1;
+#pragma unroll 1
+        for (int nu = 0; nu < 4; nu++) {
+            if (nu == mu) continue;
+            const int b_nu = step_offset(g, n, nu, -1);
+            if (MEAS && meas_takes(mu, nu)) {
+                // the plane this link takes for the measurement: S_up and S_low
+                // separately, W = S_up - S_low, the parts P(U W) at n and P(W U) at n + mu
+                M3<T> W;
+                if (nu > mu) {
+                    const int s_nup = (n.lex + step_offset(g, n, nu, +1)) >> 1;
+                    const M3<T> t = mul_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
+                    T *slot = my + 18 * kSiteBlock * tslot(mu, nu);
+#pragma unroll
+                    for (int e = 0; e < 9; e++) {
+                        slot[(2 * e) * kSiteBlock] = t.e[e].re;
+                        slot[(2 * e + 1) * kSiteBlock] = t.e[e].im;
+                    }
+                    W = mul_nd(t, in.load(nu, p, s));
+                } else {
+                    const T *slot = my + 18 * kSiteBlock * tslot(nu, mu);
+                    M3<T> t;
+#pragma unroll
+                    for (int e = 0; e < 9; e++) {
+                        t.e[e].re = slot[(2 * e) * kSiteBlock];
+                        t.e[e].im = slot[(2 * e + 1) * kSiteBlock];
+                    }
+                    W = mul_dd(t, in.load(nu, p, s));
+                }
+                add_to(A, W);
+                plaq += retr_mul(in.load(mu, p, s), W);  // ReTr(U S_up)
+                asm volatile("" ::: "memory");
+                {
+                    const int s_num = (n.lex + b_nu) >> 1, s_diag = (n.lex + f_mu + b_nu) >> 1;
+                    M3<T> t = mul_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
+                    const M3<T> S = mul(t, in.load(nu, q, s_num));
+                    add_to(A, S);
+                    sub_from(W, S);
+                }
+                const bool neg = nu < mu;
+                const int pl = neg ? plane_of(nu, mu) : plane_of(mu, nu);
+                asm volatile("" ::: "memory");
+                cp->ah.store(2 * pl, p, s, ah_neg_if(proj_ah8(mul(in.load(mu, p, s), W)), neg));
+                asm volatile("" ::: "memory");
+                cp->ah.store(2 * pl + 1, q, s_mu, ah_neg_if(proj_ah8(mul(W, in.load(mu, p, s))), neg));
+                continue;
+            }
+            if (nu > mu) {
+                const int s_nup = (n.lex + step_offset(g, n, nu, +1)) >> 1;
+                const M3<T> t = mul_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
+                T *slot = my + 18 * kSiteBlock * tslot(mu, nu);
+#pragma unroll
+                for (int e = 0; e < 9; e++) {
+                    slot[(2 * e) * kSiteBlock] = t.e[e].re;
+                    slot[(2 * e + 1) * kSiteBlock] = t.e[e].im;
+                }
+                acc_mul_nd(A, t, in.load(nu, p, s));
+            } else {
+                const T *slot = my + 18 * kSiteBlock * tslot(nu, mu);
+                M3<T> t;
+#pragma unroll
+                for (int e = 0; e < 9; e++) {
+                    t.e[e].re = slot[(2 * e) * kSiteBlock];
+                    t.e[e].im = slot[(2 * e + 1) * kSiteBlock];
+                }
+                acc_mul_dd(A, t, in.load(nu, p, s));  // T_numu^+ U_nu(n)^+ = U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+
+            }
+            {
+                const int s_num = (n.lex + b_nu) >> 1, s_diag = (n.lex + f_mu + b_nu) >> 1;
+                M3<T> t = mul_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
+                acc_mul(A, t, in.load(nu, q, s_num));
+            }
+        }
+        if (MEAS) cp->plaq[(mu * 2 + p) * g.Vh + s] = plaq;
+        const M3<T> U = in.load(mu, p, s);
+        const AH8<T> Z = project_ah(mul(U, A));
+        AH8<T> M;
+        if (STAGE == 0) {
+            M = ah_scale(alpha, Z);
+            zf.store(mu, p, s, Z);
+        } else {
+            const AH8<T> W = zf.load(mu, p, s);
+            M = ah_axpby(alpha, Z, beta, W);
+            if (STAGE == 1) zf.store(mu, p, s, M);
+        }
+        if (KIND == EXP_MORNINGSTAR) out.store(mu, p, s, mul_plus_right(expm_morningstar<T, true>(M), U));
+        else out.store(mu, p, s, mul(expm<T>(KIND, M), U));
+    }
+}
+
+template <typename T, int KIND, int STAGE>
+__global__ void __launch_bounds__(kSiteBlock) k_flow_stage_site(Geom g, LinkField<T> in, LinkField<T> out,
+                                                                ForceField<T> zf, T alpha, T beta) {
+    __shared__ T slots[4 * 18 * kSiteBlock];
+    flow_stage_site_body<T, KIND, STAGE>(g, in, out, zf, alpha, beta, blockIdx.x, slots);
+}
+
 // One __global__ per register cap (none: the compiler's own choice under
 // 128-thread launch bounds) and site-block shape; the autotuner picks among
 // them per lattice.
@@ -100,7 +238,7 @@ GLAC_FLOW_KERNEL(k_flow_stage_r96, __maxnreg__(96))
 // Register caps per variant ([fp64, fp32]; 0 = no cap, -1 = unused slot); the
 // flow family also varies the site-block shape.
 const int kFlowRegs[2][kMaxVariants] = {{0, 128, 0, 128}, {0, 80, 0, 96}};
-const int kFlowShape[2][kMaxVariants] = {{0, 0, 1, 2}, {0, 0, 1, 0}};
+const int kFlowShape[2][kMaxVariants] = {{0, 0, 1, 2}, {0, 0, 3, 0}};
 const int kMetroRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 96, 80, 128}};
 const int kObsRegs[2][kMaxVariants] = {{0, 128, -1, -1}, {0, 128, 168, -1}};
 
@@ -144,6 +282,13 @@ static void flow_dispatch_caps(int regs, cudaStream_t st, const Geom &g, const L
 template <typename T, int KIND, int STAGE>
 static void flow_dispatch(int regs, int shape, cudaStream_t st, const Geom &g, const LinkField<T> &in,
                           const LinkField<T> &out, const ForceField<T> &zf, T a, T b) {
+    if constexpr (sizeof(T) == 4) {
+        if (shape == 3) {
+            const dim3 grid(2 * ((g.Vh + kSiteBlock - 1) / kSiteBlock));
+            k_flow_stage_site<T, KIND, STAGE><<<grid, kSiteBlock, 0, st>>>(g, in, out, zf, a, b);
+            return;
+        }
+    }
     if (shape == 1) {
         const dim3 grid((g.Vh + 15) / 16);
         k_flow_stage<T, KIND, STAGE, 1><<<grid, 128, 0, st>>>(g, in, out, zf, a, b);
@@ -315,11 +460,31 @@ GLAC_FLOW_MEAS_KERNEL(k_flow_stage0_meas, __launch_bounds__(128))
 GLAC_FLOW_MEAS_KERNEL(k_flow_stage0_meas_r128, __maxnreg__(128))
 #undef GLAC_FLOW_MEAS_KERNEL
 
+// The site-per-thread form (shape 3 of the flow stage) with the measurement.
+template <typename T, int KIND>
+__global__ void __launch_bounds__(kSiteBlock) k_flow_stage0_meas_site(Geom g, LinkField<T> in, LinkField<T> out,
+                                                                      ForceField<T> zf, CloverParts<T> cp, T alpha) {
+    __shared__ T slots[4 * 18 * kSiteBlock];
+    flow_stage_site_body<T, KIND, 0, true>(g, in, out, zf, alpha, T(0), blockIdx.x, slots, &cp);
+}
+
 template <typename T>
 void launch_flow_stage0_meas(const Geom &g, const LinkField<T> &in, const LinkField<T> &out, const ForceField<T> &zf,
                              const CloverParts<T> &cp, int kind, double alpha, int regs, cudaStream_t st) {
     const dim3 grid(8 * ((g.Vh + 127) / 128));
     const T a = (T)alpha;
+    if constexpr (sizeof(T) == 4) {
+        if (regs == 3) {  // the site-per-thread form
+            const dim3 gs(2 * ((g.Vh + kSiteBlock - 1) / kSiteBlock));
+            switch (kind) {
+            case 0: k_flow_stage0_meas_site<T, 0><<<gs, kSiteBlock, 0, st>>>(g, in, out, zf, cp, a); return;
+            case 1: k_flow_stage0_meas_site<T, 1><<<gs, kSiteBlock, 0, st>>>(g, in, out, zf, cp, a); return;
+            case 2: k_flow_stage0_meas_site<T, 2><<<gs, kSiteBlock, 0, st>>>(g, in, out, zf, cp, a); return;
+            case 3: k_flow_stage0_meas_site<T, 3><<<gs, kSiteBlock, 0, st>>>(g, in, out, zf, cp, a); return;
+            default: throw std::invalid_argument("bad exp kind");
+            }
+        }
+    }
 #define GLAC_MEAS_CASE(K)                                                                                 \
     if (kind == K) {                                                                                      \
         if (regs == 128) k_flow_stage0_meas_r128<T, K><<<grid, 128, 0, st>>>(g, in, out, zf, cp, a);        \
@@ -972,6 +1137,25 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 3) k_flow_stage1_com
     obs_block_reduce(plaq, en, qt, partial, (t * 2 + p) * nb + j);
 }
 
+// The same with the site-per-thread stage (FP32 shape 3): every block covers
+// 128 consecutive sites of one parity, does their four links' stage-1 update,
+// then combines and reduces the measurement parts of those sites.
+template <typename T, int KIND>
+__global__ void __launch_bounds__(kSiteBlock) k_flow_stage1_combine_site(Geom g, LinkField<T> in, LinkField<T> out,
+                                                                         ForceField<T> zf, T alpha, T beta,
+                                                                         CloverParts<T> cp, double *partial) {
+    __shared__ T slots[4 * 18 * kSiteBlock];
+    flow_stage_site_body<T, KIND, 1>(g, in, out, zf, alpha, beta, blockIdx.x, slots);
+    const int p = blockIdx.x & 1;
+    const int s0 = (blockIdx.x >> 1) * kSiteBlock, s = s0 + threadIdx.x;
+    const int half_slice = g.Vh / g.N[3];
+    const int nb = half_slice >> 7;
+    const int t = s0 / half_slice, j = (s0 - t * half_slice) >> 7;
+    double plaq = 0.0, en = 0.0, qt = 0.0;
+    combine_site(g, cp, p, s, plaq, en, qt);
+    obs_block_reduce(plaq, en, qt, partial, (t * 2 + p) * nb + j);
+}
+
 bool obs_combine_in_stage1(const Geom &g, const ObsPlan &plan) {
     const int half_slice = g.Vh / g.N[3];
     return half_slice % 128 == 0 && plan.Bv == 128 && plan.nb == half_slice / 128;
@@ -981,11 +1165,25 @@ template <typename T>
 void launch_flow_stage1_combine(const Geom &g, const LinkField<T> &in, const LinkField<T> &out,
                                 const ForceField<T> &zf, int kind, double alpha, double beta,
                                 const CloverParts<T> &cp, const ObsPlan &plan, double *partial, double *obs_out,
-                                cudaStream_t st) {
+                                bool site, cudaStream_t st) {
     if (g.N[3] > 1024) throw std::invalid_argument("Nt > 1024 not supported by the observable reduction");
     if (!obs_combine_in_stage1(g, plan)) throw std::invalid_argument("lattice does not allow the stage-1 combine");
     const dim3 grid(8 * (g.Vh / 128));
     const T a = (T)alpha, b = (T)beta;
+    if constexpr (sizeof(T) == 4) {
+        if (site) {
+            const dim3 gs(2 * (g.Vh / kSiteBlock));
+            switch (kind) {
+            case 0: k_flow_stage1_combine_site<T, 0><<<gs, kSiteBlock, 0, st>>>(g, in, out, zf, a, b, cp, partial); break;
+            case 1: k_flow_stage1_combine_site<T, 1><<<gs, kSiteBlock, 0, st>>>(g, in, out, zf, a, b, cp, partial); break;
+            case 2: k_flow_stage1_combine_site<T, 2><<<gs, kSiteBlock, 0, st>>>(g, in, out, zf, a, b, cp, partial); break;
+            case 3: k_flow_stage1_combine_site<T, 3><<<gs, kSiteBlock, 0, st>>>(g, in, out, zf, a, b, cp, partial); break;
+            default: throw std::invalid_argument("bad exp kind");
+            }
+            k_obs_finalize<<<1, 1024, 0, st>>>(g.N[3], plan.nb, g.V, partial, obs_out);
+            return;
+        }
+    }
     switch (kind) {
     case 0: k_flow_stage1_combine<T, 0><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, cp, partial); break;
     case 1: k_flow_stage1_combine<T, 1><<<grid, 128, 0, st>>>(g, in, out, zf, a, b, cp, partial); break;
@@ -998,11 +1196,11 @@ void launch_flow_stage1_combine(const Geom &g, const LinkField<T> &in, const Lin
 template void launch_flow_stage1_combine<double>(const Geom &, const LinkField<double> &, const LinkField<double> &,
                                                  const ForceField<double> &, int, double, double,
                                                  const CloverParts<double> &, const ObsPlan &, double *, double *,
-                                                 cudaStream_t);
+                                                 bool, cudaStream_t);
 template void launch_flow_stage1_combine<float>(const Geom &, const LinkField<float> &, const LinkField<float> &,
                                                 const ForceField<float> &, int, double, double,
                                                 const CloverParts<float> &, const ObsPlan &, double *, double *,
-                                                cudaStream_t);
+                                                bool, cudaStream_t);
 
 template <typename T>
 void launch_obs_combine(const Geom &g, const CloverParts<T> &cp, const ObsPlan &plan, double *partial, double *out,

@@ -93,7 +93,7 @@ template <typename T>
 void launch_flow_stage1_combine(const Geom &g, const LinkField<T> &in, const LinkField<T> &out,
                                 const ForceField<T> &zf, int kind, double alpha, double beta,
                                 const CloverParts<T> &cp, const ObsPlan &plan, double *partial, double *obs_out,
-                                cudaStream_t st);
+                                bool site, cudaStream_t st);
 // whether the 12 clover-part slots of a lattice fit 32-bit element offsets
 inline bool clover_offsets_fit(long long V, bool fp64) {
     const long long vh32 = ((V / 2) + 31) / 32 * 32;

@@ -154,6 +154,19 @@ template <typename R> GLAC_HD void acc_mul_nd(M3<R> &Acc, const M3<R> &A, const 
             Acc(i, j) = s;
         }
 }
+// Acc += A^+ B^+  (fused accumulate, no temporary)
+template <typename R> GLAC_HD void acc_mul_dd(M3<R> &Acc, const M3<R> &A, const M3<R> &B) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            Cx<R> s = Acc(i, j);
+            s = cmac_cc(s, A(0, i), B(j, 0));
+            s = cmac_cc(s, A(1, i), B(j, 1));
+            s = cmac_cc(s, A(2, i), B(j, 2));
+            Acc(i, j) = s;
+        }
+}
 // Acc += A B
 // D U + U with each element's small sum D(i,:) U(:,j) formed first and U(i,j)
 // added last (one rounding at the magnitude of U); column by column, so a
