@@ -345,10 +345,13 @@ def run_gpu(args):
 
     obs_buf = np.empty((args.steps + 1, 3 + DIMS[3]))
 
-    L.flow(args.warmup, measure=True)
-    n0 = L.launch_count
+    # clocks sampled from the warm-up through the timed region (nvidia-smi needs
+    # a moment to start, and the timed region lasts tens of milliseconds)
     clk = ClockSampler(local)
     clk.start()
+    time.sleep(0.5)
+    L.flow(args.warmup, measure=True)
+    n0 = L.launch_count
     # timed: K RK3 steps, each followed by the observable measurement (device
     # buffer), all K+1 observable vectors copied back at the end
     t_main = timed(lambda: L.flow(args.steps, out=obs_buf), 1)
@@ -368,6 +371,8 @@ def run_gpu(args):
     reps = max(3, min(args.steps, 20))
     clk_st = ClockSampler(local)
     clk_st.start()
+    time.sleep(0.5)
+    reps = max(reps, 100)  # long enough for several clock samples
     stm = np.array(L.flow_stage_times_measured(reps))
     st = np.array(L.flow_stage_times(reps))
     stage_clocks = clk_st.stop()
@@ -489,11 +494,15 @@ def run_gpu(args):
             _, _, sec_sweeps = E.run(100, 0)
             E.run(0, 200)
             _, _, sec_flow = E.run(0, 200)
+            # the whole schedule as one persistent cooperative launch
+            E.run_persistent(100, 200)
+            _, obs_p, sec_p = E.run_persistent(100, 200)
         sites_e = int(sum(np.prod(d) for d in dims_l))
         ens_extra = {"lattices": 64, "sites": sites_e, "schedule": "100 sweeps + 200 flow steps with observables",
                      "graph_gpu_s": sec_e,
                      "sweeps_graph_gpu_s": sec_sweeps, "link_updates_per_s": 4 * sites_e * 100 / sec_sweeps,
                      "flow_graph_gpu_s": sec_flow, "flow_site_steps_per_s": sites_e * 200 / sec_flow,
+                     "persistent_launch_gpu_s": sec_p,
                      "autotune_chosen": tune_e["chosen"], "plaq_after_flow_mean": float(np.mean([o[-1, 0] for o in obs_e]))}
 
     line = {

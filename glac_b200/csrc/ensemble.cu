@@ -17,6 +17,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -55,6 +56,9 @@ struct glac_ensemble {
     bool flips = true;
     bool has_field = false;
     int tune[3] = {0, 0, 0};
+    GridBarrier *barrier = nullptr;             // the persistent launch's grid barrier (first use)
+    unsigned long long persistent_wait_ns = 5000000000ull;  // its wait limit (5 s)
+    int persistent_test_stall = 0;              // test mode: one block never arrives
     uint64_t launches = 0;
     std::string err;
 };
@@ -397,7 +401,7 @@ void glac_ensemble_destroy(glac_ensemble *E) {
     if (E->stream) cudaStreamSynchronize(E->stream);
     drop_graph(E);
     for (void *p : {E->field[0], E->field[1], E->field[2], E->force, (void *)E->partial, E->slots, (void *)E->acc,
-                    (void *)E->sweep_dev, (void *)E->obs, (void *)E->staging, E->clover})
+                    (void *)E->sweep_dev, (void *)E->obs, (void *)E->staging, E->clover, (void *)E->barrier})
         if (p) cudaFree(p);
     for (int k = 0; k < ENS_NPHASE; k++)
         if (E->start[k]) cudaFree(E->start[k]);
@@ -414,6 +418,14 @@ glac_status glac_ensemble_set_option(glac_ensemble *E, const char *key, long val
     if (std::string(key) == "su2_sign_flips" && (value == 0 || value == 1)) {
         E->flips = value != 0;
         drop_graph(E);
+        return GLAC_OK;
+    }
+    if (std::string(key) == "persistent_wait_ms" && value > 0 && value <= 60000) {
+        E->persistent_wait_ns = (unsigned long long)value * 1000000ull;
+        return GLAC_OK;
+    }
+    if (std::string(key) == "persistent_test_stall" && (value == 0 || value == 1)) {
+        E->persistent_test_stall = (int)value;
         return GLAC_OK;
     }
     if (std::string(key) == "fused_measure" && (value == 0 || value == 1)) {
@@ -557,6 +569,83 @@ glac_status glac_ensemble_run(glac_ensemble *E, int n_sweeps, int n_steps, doubl
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         E->launches += 8ull * n_sweeps + 1 + (n_steps >= 0 ? 2 + 5ull * n_steps : 0);
+        E->sweep += (uint32_t)n_sweeps;
+        if (gpu_seconds) *gpu_seconds = ms * 1e-3;
+        if (acceptance) read_acceptance(E, n_sweeps, acceptance);
+        if (obs) read_obs(E, n_steps, obs);
+        return GLAC_OK;
+    });
+}
+
+glac_status glac_ensemble_run_persistent(glac_ensemble *E, int n_sweeps, int n_steps, double *acceptance,
+                                         double *obs, double *gpu_seconds) {
+    return eguarded(E, [&] {
+        glac_status s = need_field(E);
+        if (s != GLAC_OK) return s;
+        if (n_sweeps < 0 || n_steps < 0) { E->err = "negative count"; return GLAC_ERR_ARG; }
+        if (E->d.precision != GLAC_FP32 || !E->clover || !E->fused_measure) {
+            E->err = "the persistent launch runs FP32 ensembles with the measurement inside flow stage 0";
+            return GLAC_ERR_STATE;
+        }
+        int coop = 0, sms = 0;
+        eck(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, E->d.device), "attribute");
+        eck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->d.device), "attribute");
+        const int per_sm = persistent_blocks_per_sm();
+        if (!coop || per_sm <= 0) {
+            E->err = "cooperative launch not available for the persistent kernel on this device";
+            return GLAC_ERR_CUDA;
+        }
+        ensure_obs(E, n_steps);
+        if (!E->barrier) eck(cudaMalloc(&E->barrier, sizeof(GridBarrier)), "barrier alloc");
+        eck(cudaMemsetAsync(E->barrier, 0, sizeof(GridBarrier), E->stream), "memset");
+        eck(cudaMemsetAsync(E->acc, 0, E->M * sizeof(unsigned long long), E->stream), "memset");
+        const double eps = E->d.flow_eps;
+        EnsSchedule sc;
+        std::memset(&sc, 0, sizeof(sc));
+        sc.M = E->M;
+        sc.n_sweeps = n_sweeps;
+        sc.n_steps = n_steps;
+        sc.start_metro = E->start[ENS_METRO];
+        sc.start_flow0 = E->start[ENS_FLOW0];
+        sc.start_obs = E->start[ENS_OBS];
+        sc.nb_metro = E->nblk[ENS_METRO];
+        sc.nb_flow0 = E->nblk[ENS_FLOW0];
+        sc.nb_obs = E->nblk[ENS_OBS];
+        sc.eps = E->d.su3_eps;
+        sc.sq1me = std::sqrt(1.0 - E->d.su3_eps * E->d.su3_eps);
+        const double alpha[3] = {eps * 0.25, eps * 0.8888888888888888, 0.75 * eps};
+        const double beta[3] = {0.0, -(eps * 0.4722222222222222), -1.0};
+        for (int k = 0; k < 3; k++) { sc.alpha[k] = alpha[k]; sc.beta[k] = beta[k]; }
+        sc.nhits = E->d.n_updates;
+        sc.k0 = (uint32_t)E->d.seed;
+        sc.k1 = (uint32_t)(E->d.seed >> 32);
+        sc.sweep_base = E->sweep_dev;
+        sc.flips = E->flips;
+        sc.chain = E->field[0];
+        sc.flow = E->field[1];
+        sc.field_words = E->field_total / 16;
+        sc.wait_ns = E->persistent_wait_ns;
+        sc.test_skip_block0 = E->persistent_test_stall;
+        cudaEvent_t e0, e1;
+        eck(cudaEventCreate(&e0), "event");
+        eck(cudaEventCreate(&e1), "event");
+        eck(cudaEventRecord(e0, E->stream), "event");
+        eck(launch_ens_persistent(static_cast<const LatSlot<float> *>(E->slots), sc, E->barrier, per_sm * sms,
+                                  E->stream),
+            "persistent launch");
+        eck(cudaEventRecord(e1, E->stream), "event");
+        eck(cudaEventSynchronize(e1), "sync");
+        float ms = 0.f;
+        eck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        E->launches += 1;
+        GridBarrier b;
+        eck(cudaMemcpy(&b, E->barrier, sizeof(b), cudaMemcpyDeviceToHost), "D2H barrier");
+        if (b.err) {
+            E->err = "a grid barrier of the persistent launch waited past its limit; the fields are undefined";
+            return GLAC_ERR_TIMEOUT;
+        }
         E->sweep += (uint32_t)n_sweeps;
         if (gpu_seconds) *gpu_seconds = ms * 1e-3;
         if (acceptance) read_acceptance(E, n_sweeps, acceptance);

@@ -1915,6 +1915,170 @@ void launch_ens_obs_combine(const LatSlot<T> *slots, const int *start, int nbloc
     kb_obs_finalize<T><<<M, 1024, 0, st>>>(slots, meas);
 }
 
+// ---------------------------------------------------------------------------
+// The whole ensemble schedule in one persistent launch (FP32): every block of
+// a cooperative grid (all co-resident) walks the virtual blocks of each phase
+// in turn -- the 8 Metropolis sub-sweeps of every sweep, the chain -> flow copy,
+// and per flow step stage 0 with the measurement's parts, their combination,
+// the per-lattice reduction, stages 1 and 2 -- with a grid-wide barrier between
+// phases.  The barrier waits at most wait_ns of the GPU's global timer; when a
+// wait runs out the barrier records the error, every block leaves at its next
+// barrier, and the host reports a timeout (the field is then undefined).
+// test_skip_block0: block 0 leaves at the first barrier without arriving, so
+// the others' waits run out (the failure path, without a fault or a hang).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t gtimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// false: a wait ran out here or elsewhere (the caller leaves)
+__device__ bool grid_barrier(GridBarrier *b, uint64_t wait_ns) {
+    __shared__ int ok_sh;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile unsigned int *vgen = &b->gen;
+        volatile int *verr = &b->err;
+        const unsigned int gen = *vgen;
+        __threadfence();
+        if (atomicAdd(&b->count, 1u) + 1u == gridDim.x) {
+            atomicExch(&b->count, 0u);
+            __threadfence();
+            atomicAdd(&b->gen, 1u);
+        } else {
+            // bounded by the global timer, and by a count of tries as a second
+            // bound (a try reads L2 and sleeps, well over 16 ns, so wait_ns / 16
+            // tries outlast wait_ns)
+            const uint64_t t0 = gtimer_ns();
+            for (uint64_t it = 0; *vgen == gen; it++) {
+                if (*verr) { ok = 0; break; }
+                if (gtimer_ns() - t0 > wait_ns || it > (wait_ns >> 4)) {
+                    atomicExch(&b->err, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (*verr) ok = 0;
+        ok_sh = ok;
+    }
+    __syncthreads();
+    return ok_sh != 0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128, 4) kb_persistent(const LatSlot<T> *__restrict__ slots, EnsSchedule sc,
+                                                        GridBarrier *bar) {
+    const int M = sc.M;
+    const uint32_t sweep0 = *sc.sweep_base;  // advanced at the end, after the last barrier
+    Proposal P;
+    P.flips = sc.flips;
+    bool ok = true;
+    if (sc.test_skip_block0 && blockIdx.x == 0) return;
+    // Metropolis: 8 (mu, parity) sub-sweeps per sweep on the chain fields
+    for (int i = 0; i < sc.n_sweeps && ok; i++)
+        for (int k = 0; k < 8 && ok; k++) {
+            for (int vb = blockIdx.x; vb < sc.nb_metro; vb += gridDim.x) {
+                const int l = slot_of(sc.start_metro, M, vb);
+                const LatSlot<T> &S = slots[l];
+                metropolis_body<T, false>(S.g, S.f[0], k >> 1, k & 1, (T)(-S.beta / 3.f), (T)sc.eps, (T)sc.sq1me,
+                                          sc.nhits, sc.k0, sc.k1, sweep0 + (uint32_t)i, S.stream, S.acc, P, S.beta,
+                                          vb - __ldg(sc.start_metro + l));
+            }
+            ok = grid_barrier(bar, sc.wait_ns);
+        }
+    if (sc.n_steps < 0) {
+        if (ok && blockIdx.x == 0 && threadIdx.x == 0) *sc.sweep_base = sweep0 + (uint32_t)sc.n_sweeps;
+        return;
+    }
+    // the flow fields from the chains (one allocation per role, equal offsets)
+    if (ok) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(sc.chain);
+        uint4 *dst = reinterpret_cast<uint4 *>(sc.flow);
+        for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < sc.field_words;
+             w += (size_t)gridDim.x * blockDim.x)
+            dst[w] = src[w];
+        ok = grid_barrier(bar, sc.wait_ns);
+    }
+    int cur = 1;
+    for (int step = 0; step < sc.n_steps && ok; step++) {
+        // stage 0 with the parts of the measurement of the field before the step
+        for (int vb = blockIdx.x; vb < sc.nb_flow0 && ok; vb += gridDim.x) {
+            const int l = slot_of(sc.start_flow0, M, vb);
+            const LatSlot<T> &S = slots[l];
+            flow_stage0_meas_body<T, EXP_MORNINGSTAR>(S.g, S.f[cur], S.f[3 - cur], S.z, S.cp, (T)sc.alpha[0],
+                                                      vb - __ldg(sc.start_flow0 + l));
+        }
+        if (ok) ok = grid_barrier(bar, sc.wait_ns);
+        for (int vb = blockIdx.x; vb < sc.nb_obs && ok; vb += gridDim.x) {
+            const int l = slot_of(sc.start_obs, M, vb);
+            const LatSlot<T> &S = slots[l];
+            const int b = vb - __ldg(sc.start_obs + l);
+            const int t = b / (2 * S.nb), p = (b / S.nb) & 1, j = b % S.nb;
+            const int half_slice = S.g.Vh / S.g.N[3];
+            const bool valid = (int)threadIdx.x < S.Bv;
+            const int s = t * half_slice + j * S.Bv + (valid ? (int)threadIdx.x : 0);
+            double plaq = 0.0, en = 0.0, qt = 0.0;
+            if (valid) combine_site(S.g, S.cp, p, s, plaq, en, qt);
+            obs_block_reduce(plaq, en, qt, S.partial, b);
+        }
+        if (ok) ok = grid_barrier(bar, sc.wait_ns);
+        for (int l = blockIdx.x; l < M && ok; l += gridDim.x) {
+            const LatSlot<T> &S = slots[l];
+            obs_finalize_body(S.g.N[3], S.nb, S.g.V, S.partial, S.obs + (size_t)step * (3 + S.g.N[3]));
+        }
+        // (the finalize reads the partials the combine wrote; the next phases do not touch them)
+        for (int st = 1; st < 3 && ok; st++) {
+            const int src = st == 1 ? 3 - cur : cur, dstf = st == 1 ? cur : 3 - cur;
+            for (int vb = blockIdx.x; vb < sc.nb_flow0; vb += gridDim.x) {
+                const int l = slot_of(sc.start_flow0, M, vb);
+                const LatSlot<T> &S = slots[l];
+                if (st == 1)
+                    flow_stage_body<T, EXP_MORNINGSTAR, 1, 0>(S.g, S.f[src], S.f[dstf], S.z, (T)sc.alpha[1],
+                                                              (T)sc.beta[1], vb - __ldg(sc.start_flow0 + l));
+                else
+                    flow_stage_body<T, EXP_MORNINGSTAR, 2, 0>(S.g, S.f[src], S.f[dstf], S.z, (T)sc.alpha[2],
+                                                              (T)sc.beta[2], vb - __ldg(sc.start_flow0 + l));
+            }
+            ok = grid_barrier(bar, sc.wait_ns);
+        }
+        cur = 3 - cur;  // three stages: the field ends in the other buffer
+    }
+    // the last measurement as a pass of its own
+    if (ok) {
+        for (int vb = blockIdx.x; vb < sc.nb_obs; vb += gridDim.x) {
+            const int l = slot_of(sc.start_obs, M, vb);
+            const LatSlot<T> &S = slots[l];
+            observables_body<T>(S.g, S.f[cur], S.nb, S.Bv, S.partial, vb - __ldg(sc.start_obs + l));
+        }
+        ok = grid_barrier(bar, sc.wait_ns);
+    }
+    if (ok) {
+        for (int l = blockIdx.x; l < M; l += gridDim.x) {
+            const LatSlot<T> &S = slots[l];
+            obs_finalize_body(S.g.N[3], S.nb, S.g.V, S.partial, S.obs + (size_t)sc.n_steps * (3 + S.g.N[3]));
+        }
+        ok = grid_barrier(bar, sc.wait_ns);
+    }
+    if (ok && blockIdx.x == 0 && threadIdx.x == 0) *sc.sweep_base = sweep0 + (uint32_t)sc.n_sweeps;
+}
+
+int persistent_blocks_per_sm() {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_persistent<float>, 128, 0) != cudaSuccess) return 0;
+    return nb;
+}
+
+cudaError_t launch_ens_persistent(const LatSlot<float> *slots, const EnsSchedule &sc, GridBarrier *bar, int grid,
+                                  cudaStream_t st) {
+    void *args[] = {(void *)&slots, (void *)&sc, (void *)&bar};
+    return cudaLaunchCooperativeKernel((const void *)kb_persistent<float>, dim3(grid), dim3(128), args, 0, st);
+}
+
 __global__ void k_advance(uint32_t *counter, uint32_t by) { counter[0] += by; }
 void launch_advance(uint32_t *counter, uint32_t by, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(counter, by); }
 

@@ -197,4 +197,29 @@ void launch_ens_obs_combine(const LatSlot<T> *slots, const int *start, int nbloc
                             cudaStream_t st);
 void launch_advance(uint32_t *counter, uint32_t by, cudaStream_t st);
 
+// The whole schedule in one persistent cooperative launch (FP32; measurement
+// inside stage 0).  A barrier's state, zeroed before the launch.
+struct GridBarrier {
+    unsigned int count, gen;
+    int err;
+};
+struct EnsSchedule {
+    int M, n_sweeps, n_steps;  // n_steps < 0: sweeps only
+    const int *start_metro, *start_flow0, *start_obs;
+    int nb_metro, nb_flow0, nb_obs;
+    double eps, sq1me, alpha[3], beta[3];
+    int nhits;
+    uint32_t k0, k1;
+    uint32_t *sweep_base;
+    bool flips;
+    const void *chain;  // field role 0 and 1 base pointers, field_words 16-byte words
+    void *flow;
+    size_t field_words;
+    unsigned long long wait_ns;
+    int test_skip_block0;
+};
+int persistent_blocks_per_sm();
+cudaError_t launch_ens_persistent(const LatSlot<float> *slots, const EnsSchedule &sc, GridBarrier *bar, int grid,
+                                  cudaStream_t st);
+
 }  // namespace glac

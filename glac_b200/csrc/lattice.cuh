@@ -141,6 +141,11 @@ inline bool field_offsets_fit(long long V, bool fp64) {
     return (fp64 ? 72 : 32) * vh32 < (1ll << 32);
 }
 
+// Field loads are plain global loads (L1-cached), not the non-coherent
+// read-only path (__ldg): the persistent ensemble kernel reads, after a grid
+// barrier, links that other blocks wrote earlier in the same launch, which the
+// non-coherent path does not guarantee to see.  (Timed on B200 at 32^3 x 64:
+// flow steps and Metropolis sweeps within 2 % of the __ldg build, either way.)
 template <typename T> struct LinkField;
 
 template <> struct LinkField<double> {
@@ -154,7 +159,7 @@ template <> struct LinkField<double> {
         M3<double> U;
 #pragma unroll
         for (int k = 0; k < 9; k++) {
-            double2 v = __ldg(b + 32 * k);
+            double2 v = b[32 * k];
             U.e[k].re = v.x; U.e[k].im = v.y;
         }
         return U;
@@ -189,10 +194,10 @@ template <> struct LinkField<float> {
         M3<float> U;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            float4 v = __ldg(b + 32 * k);
+            float4 v = b[32 * k];
             U.e[2 * k].re = v.x; U.e[2 * k].im = v.y; U.e[2 * k + 1].re = v.z; U.e[2 * k + 1].im = v.w;
         }
-        float2 w = __ldg(p2 + at2(mu, par, s));
+        float2 w = p2[at2(mu, par, s)];
         U.e[8].re = w.x; U.e[8].im = w.y;
         return U;
     }

@@ -53,6 +53,7 @@ def _bind(L):
     L.glac_ensemble_obs_count.restype = C.c_longlong
     L.glac_ensemble_flow.argtypes = [P, C.c_int, C.c_void_p]
     L.glac_ensemble_run.argtypes = [P, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
+    L.glac_ensemble_run_persistent.argtypes = [P, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
     L.glac_ensemble_autotune.argtypes = [P, C.c_int, C.c_void_p]
     L.glac_ensemble_get_tuning.argtypes = [P, C.c_void_p]
     L.glac_ensemble_set_tuning.argtypes = [P, C.c_void_p]
@@ -166,6 +167,16 @@ class Ensemble:
         sec = C.c_double(0.0)
         self._ck(lib().glac_ensemble_run(self._h, int(n_sweeps), int(n_steps), acc.ctypes.data, flat.ctypes.data,
                                          C.byref(sec)))
+        return acc, self._split(flat, n_steps), sec.value
+
+    def run_persistent(self, n_sweeps, n_steps):
+        """The same schedule as run(), as one persistent cooperative launch (FP32):
+        (acceptance, per-lattice measurements, GPU seconds)."""
+        acc = np.empty(self.n)
+        flat = np.empty(lib().glac_ensemble_obs_count(self._h, int(n_steps)))
+        sec = C.c_double(0.0)
+        self._ck(lib().glac_ensemble_run_persistent(self._h, int(n_sweeps), int(n_steps), acc.ctypes.data,
+                                                    flat.ctypes.data, C.byref(sec)))
         return acc, self._split(flat, n_steps), sec.value
 
     def autotune(self, reps=2):

@@ -329,6 +329,15 @@ glac_status glac_ensemble_flow(glac_ensemble *ens, int n_steps, double *obs);
  * gpu_seconds (may be NULL) = device time of the graph. */
 glac_status glac_ensemble_run(glac_ensemble *ens, int n_sweeps, int n_steps, double *acceptance, double *obs,
                               double *gpu_seconds);
+/* The same schedule as one persistent cooperative launch (FP32 ensembles with
+ * fused_measure on): every co-resident block walks each phase's blocks in turn,
+ * with a grid-wide barrier between phases whose waits are bounded by the GPU's
+ * global timer (option "persistent_wait_ms", default 5000); a wait that runs
+ * out gives GLAC_ERR_TIMEOUT and leaves the fields undefined.  Same results as
+ * glac_ensemble_run.  "persistent_test_stall" = 1 (tests only) keeps one block
+ * from arriving, so the others' waits run out.  No reference counterpart. */
+glac_status glac_ensemble_run_persistent(glac_ensemble *ens, int n_sweeps, int n_steps, double *acceptance,
+                                         double *obs, double *gpu_seconds);
 /* Launch-variant autotuner over the whole ensemble (flow site-block shapes and
  * register caps, Metropolis and observable register caps); report[4 f + v] =
  * seconds per flow step (f = 0) / per sweep (f = 1) / per measurement (f = 2)

@@ -135,3 +135,44 @@ def test_ensemble_measurement_inside_stage0_matches_standalone(g, ens, prec, tol
         oa, ob = A.flow(4), B.flow(4)
         for i in range(len(DIMS)):
             assert_obs_close(oa[i], ob[i], 4 * tol, f"lattice {i}")
+
+
+def test_persistent_launch_equals_graph(g, ens):
+    # the whole schedule in one cooperative launch with grid barriers between
+    # the phases gives what the CUDA graph of per-phase launches gives
+    kw = dict(precision="fp32", seed=SEED, flow_eps=0.02)
+    with ens.Ensemble(DIMS, BETAS, **kw) as A, ens.Ensemble(DIMS, BETAS, **kw) as B:
+        A.hot_start(6)
+        B.hot_start(6)
+        acc_a, obs_a, _ = A.run(3, 4)
+        acc_b, obs_b, sec = B.run_persistent(3, 4)
+        assert sec > 0
+        assert np.max(np.abs(acc_a - acc_b)) < 1e-3
+        for i in range(len(DIMS)):
+            assert_obs_close(obs_b[i], obs_a[i], 1e-5, f"lattice {i}")
+            assert rel(B.get_links(i), A.get_links(i)) < 1e-5
+        # both continue the same random stream
+        acc_a, obs_a, _ = A.run(2, 1)
+        acc_b, obs_b, _ = B.run_persistent(2, 1)
+        assert np.max(np.abs(acc_a - acc_b)) < 1e-3
+
+
+def test_persistent_barrier_wait_runs_out_and_recovers(g, ens):
+    # one block held back (test mode): the others' bounded barrier waits run out,
+    # the call reports a timeout, and the ensemble works again afterwards
+    kw = dict(precision="fp32", seed=SEED, flow_eps=0.02)
+    with ens.Ensemble(DIMS, BETAS, **kw) as A, ens.Ensemble(DIMS, BETAS, **kw) as B:
+        A.hot_start(6)
+        A.set_option("persistent_wait_ms", 100)
+        A.set_option("persistent_test_stall", 1)
+        with pytest.raises(g.GlacError) as e:
+            A.run_persistent(1, 1)
+        assert e.value.status == g.GLAC_ERR_TIMEOUT
+        A.set_option("persistent_test_stall", 0)
+        A.set_option("persistent_wait_ms", 5000)
+        A.hot_start(6)
+        B.hot_start(6)
+        _, obs_a, _ = A.run_persistent(2, 2)
+        _, obs_b, _ = B.run(2, 2)
+        for i in range(len(DIMS)):
+            assert_obs_close(obs_a[i], obs_b[i], 1e-5, f"lattice {i}")
