@@ -194,8 +194,10 @@ void flow_step(glac_ctx *c, cudaEvent_t *ev = nullptr, double *meas_out = nullpt
         } else if (stage == 0 && meas_out) {
             ensure_clover(c);
             // 1: link per thread, compiler's registers; 2: the same capped at 128;
-            // 3 (FP32): site per thread, upper staple products shared
-            const int regs = c->fused_measure == 2 ? 128 : (c->fused_measure == 3 ? 3 : 0);
+            // 3 (FP32): site per thread, upper staple products shared; 4 (FP32):
+            // link per thread capped at 96 (five blocks per SM, small spill)
+            const int fm = c->fused_measure;
+            const int regs = fm == 2 ? 128 : fm == 3 ? 3 : fm == 4 ? 96 : 0;
             if (c->d.precision == GLAC_FP64) {
                 const CloverParts<double> cp = clover_view<double>(c);
                 launch_flow_stage0_meas(c->g, f64(c, src), f64(c, dst), z64(c), cp, c->d.exp_func, alpha[0], regs,
@@ -326,9 +328,9 @@ glac_status glac_sync(glac_ctx *c) {
 glac_status glac_set_option(glac_ctx *c, const char *key, long value) {
     if (!c || !key) return GLAC_ERR_ARG;
     if (std::string(key) == "fused_measure") {
-        if (value < 0 || value > 3 || (value == 3 && c->d.precision != GLAC_FP32)) {
+        if (value < 0 || value > 4 || (value >= 3 && c->d.precision != GLAC_FP32)) {
             c->err = "fused_measure takes 0 (off), 1 (on), 2 (on, 128-register kernel) or, in FP32, 3 (on, a "
-                     "thread per site)";
+                     "thread per site) or 4 (on, 96-register kernel)";
             return GLAC_ERR_ARG;
         }
         c->fused_measure = (int)value;

@@ -458,6 +458,7 @@ __device__ __forceinline__ void flow_stage0_meas_body(const Geom &g, const LinkF
     }
 GLAC_FLOW_MEAS_KERNEL(k_flow_stage0_meas, __launch_bounds__(128))
 GLAC_FLOW_MEAS_KERNEL(k_flow_stage0_meas_r128, __maxnreg__(128))
+GLAC_FLOW_MEAS_KERNEL(k_flow_stage0_meas_r96, __maxnreg__(96))
 #undef GLAC_FLOW_MEAS_KERNEL
 
 // The site-per-thread form (shape 3 of the flow stage) with the measurement.
@@ -488,6 +489,7 @@ void launch_flow_stage0_meas(const Geom &g, const LinkField<T> &in, const LinkFi
 #define GLAC_MEAS_CASE(K)                                                                                 \
     if (kind == K) {                                                                                      \
         if (regs == 128) k_flow_stage0_meas_r128<T, K><<<grid, 128, 0, st>>>(g, in, out, zf, cp, a);        \
+        else if (regs == 96) k_flow_stage0_meas_r96<T, K><<<grid, 128, 0, st>>>(g, in, out, zf, cp, a);     \
         else k_flow_stage0_meas<T, K><<<grid, 128, 0, st>>>(g, in, out, zf, cp, a);                       \
         return;                                                                                           \
     }

@@ -86,7 +86,8 @@ uint64_t glac_launch_count(const glac_ctx *ctx);
  *   from the staple pieces the stage computes anyway (two extra 3x3 products
  *   per plane instead of the ten of a separate clover pass), and the last one
  *   in a pass of its own; 1 uses the stage kernel's own register allocation, 2
- *   a 128-register variant; 0 measures every field in a pass of its own.  The
+ *   a 128-register variant, and in FP32 3 a thread per site and 4 a
+ *   96-register variant; 0 measures every field in a pass of its own.  The
  *   results are the same to rounding.
  *   "fused_combine" (default 1): with fused_measure on, the measurement's
  *   per-site combination and block reduction run inside the step's second

@@ -223,7 +223,7 @@ def test_measurement_inside_flow_stage0(g, oracle, prec, N):
         C.set_links(oracle.haar_field(N, 77))
         C.metropolis(10)
         cur = C.get_links()
-    modes = (1, 2, 3) if prec == "fp32" else (1, 2)  # kernel forms of the fused stage 0
+    modes = (1, 2, 3, 4) if prec == "fp32" else (1, 2)  # kernel forms of the fused stage 0
     with lattice(g, N, prec, flow_eps=0.02) as B:
         B.set_option("fused_measure", 0)
         for k in range(4):
