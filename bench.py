@@ -69,10 +69,10 @@ SM_COUNT, FP32_LANES_PER_SM = 148, 128
 # `python -m glac_b200.studies target`; bench.py reports it, it does not
 # re-measure it.
 EFF_Q_STUDY = {"measured_in_this_run": False, "source": "profiles/eff_q_study_32x32x32x64_b6.2.md",
-               "ratio_learned_fp32_vs_plain_fp64": 7.55, "err": 0.64,
-               "ratio_ablation_fp32_vs_plain_fp64": 8.81, "ablation_err": 0.89,
+               "ratio_learned_fp32_vs_plain_fp64": 8.06, "err": 0.63,
+               "ratio_ablation_fp32_vs_plain_fp64": 8.97, "ablation_err": 0.89,
                "estimator": "Q diffusion over 500 sweeps per second of sweeps + measurements, replica jackknife",
-               "replicas": 6, "plaquette_learned_minus_fp64_sigma": 0.4}
+               "replicas": 12, "plaquette_learned_minus_fp64_sigma": 0.6}
 # Metropolis: algorithmic bytes per link update in FP32 (9 link transfers x 72 B)
 METRO_BYTES_FP32 = 9 * 72
 
