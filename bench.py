@@ -75,6 +75,9 @@ EFF_Q_STUDY = {"measured_in_this_run": False, "source": "profiles/eff_q_study_32
                "replicas": 12, "plaquette_learned_minus_fp64_sigma": 0.6}
 # Metropolis: algorithmic bytes per link update in FP32 (9 link transfers x 72 B)
 METRO_BYTES_FP32 = 9 * 72
+# FP32 FLOP per link update (10 hits) from one ncu capture of k_metropolis_r96<float>
+# at 32^3x64: 2580 FFMA + 225 FADD + 607 FMUL per link update
+FLOPS_PER_LINK_UPDATE_METRO_FP32 = 2 * 2580 + 225 + 607
 
 
 def load_peaks():
@@ -403,6 +406,13 @@ def run_gpu(args):
                                  "frac": round(fp32_ach / fp32_peak, 4),
                                  "flops_per_site": FLOPS_PER_SITE_STAGE0_MEAS_FP32,
                                  "peak_basis": f"148 SMs x 128 FP32 lanes x 2 FLOP x {sm_mhz:.0f} MHz (median while timed)"}
+    # Metropolis on the same FP32 pipe: its FMA pipe also runs the Philox
+    # integer multiplies, so the FLOP fraction understates how busy the pipe is
+    metro_fp32 = FLOPS_PER_LINK_UPDATE_METRO_FP32 * metro_rate / world / 1e12
+    metro_fp32_pipe = {"achieved": round(metro_fp32, 2), "peak": round(fp32_peak, 2), "unit": "TFLOP/s",
+                       "frac": round(metro_fp32 / fp32_peak, 4),
+                       "flops_per_link_update": FLOPS_PER_LINK_UPDATE_METRO_FP32,
+                       "binding_unit": "FMA pipe (FP32 and Philox IMAD), 62 % busy, issue-bound (ncu)"}
     # the plain stage-0 launch (flow steps without measurement) for comparison
     plain_fp32 = FLOPS_PER_SITE_STAGE0_FP32 * V / float(st[0]) / 1e12
     roofline["unmeasured_stage0"] = {
@@ -520,7 +530,8 @@ def run_gpu(args):
             "flow_site_steps_per_s_fp64_with_obs": rate64,
             "metropolis_link_updates_per_s_fp32": metro_rate,
             "metropolis_roofline_fp32": dict(metro_roofline, peak=hbm_peak,
-                                             frac=round(metro_roofline["achieved"] / hbm_peak, 4)),
+                                             frac=round(metro_roofline["achieved"] / hbm_peak, 4),
+                                             fp32_pipe=metro_fp32_pipe),
             "metropolis_link_updates_per_s_fp64": metro64_rate,
             "learned": learned_extra,
             "eff_Q_samples_study": EFF_Q_STUDY,
