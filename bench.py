@@ -73,6 +73,13 @@ EFF_Q_STUDY = {"measured_in_this_run": False, "source": "profiles/eff_q_study_32
                "ratio_ablation_fp32_vs_plain_fp64": 8.97, "ablation_err": 0.89,
                "estimator": "Q diffusion over 500 sweeps per second of sweeps + measurements, replica jackknife",
                "replicas": 12, "plaquette_learned_minus_fp64_sigma": 0.6}
+# The study's ratio factorises as (Q diffusion per sweep, learned / plain FP64:
+# D(500) 19.2 / 5.82) x (seconds per sweep with measurements, plain FP64 /
+# learned: 9.616 / 3.933 ms).  The second factor is re-measured in every bench
+# run on the bench's own lattice (same lattice, coupling and measurement
+# schedule); the first needs chains of 10^4-10^5 sweeps and is quoted.
+EFF_Q_DIFFUSION_PER_SWEEP_RATIO = (19.2 / 5.82, 0.63 / 8.06 * 19.2 / 5.82)
+EFF_Q_SWEEPS_TIMED = 300
 # Metropolis: algorithmic bytes per link update in FP32 (9 link transfers x 72 B)
 METRO_BYTES_FP32 = 9 * 72
 # FP32 FLOP per link update (10 hits) from one ncu capture of k_metropolis_r96<float>
@@ -468,6 +475,7 @@ def run_gpu(args):
     # learned proposal spread on this lattice: ESJ data from 100 plain sweeps,
     # training on the GPU, then the learned sampler's link-updates/s
     learned_extra = None
+    eff_q_here = EFF_Q_STUDY
     if not args.no_learned:
         from glac_b200 import learned as lp
         feat, esj, plain = lp.collect_esj(L, 100, 10, 64, lp.DEFAULT_GRID, trials=4)
@@ -482,6 +490,25 @@ def run_gpu(args):
         t_l = timed(lambda: L.metropolis(1), 20)
         L.set_proposal_net(None)
         L.set_option("su2_sign_flips", 1)
+        # the second factor of the effective-Q ratio: seconds per sweep with the
+        # study's measurements (every 100 sweeps: plaquette, then Q and E of a copy
+        # flowed to t = 2) for the plain FP64 and the learned FP32 chains
+        from glac_b200 import studies
+        cfg = dict(studies.TARGET, dims=DIMS, beta=BETA,
+                   sweeps_by={"plain_fp64": EFF_Q_SWEEPS_TIMED, "learned_fp32": EFF_Q_SWEEPS_TIMED})
+        sweep_s = {}
+        for smp in ("plain_fp64", "learned_fp32"):
+            ch = studies.q_chain(start, cfg, smp, 100 + rank, params=params)
+            sweep_s[smp] = ch["wall_s"] / ch["sweeps"]
+        rate_ratio = sweep_s["plain_fp64"] / sweep_s["learned_fp32"]
+        d_ratio, d_err = EFF_Q_DIFFUSION_PER_SWEEP_RATIO
+        eff_q_here = dict(EFF_Q_STUDY,
+                          seconds_per_sweep_with_measurements_here={k: round(v, 6) for k, v in sweep_s.items()},
+                          sweeps_timed_per_sampler=EFF_Q_SWEEPS_TIMED,
+                          rate_ratio_measured_here=round(rate_ratio, 4),
+                          q_diffusion_per_sweep_ratio_from_study=round(d_ratio, 4),
+                          ratio_with_rate_measured_here=round(rate_ratio * d_ratio, 3),
+                          ratio_with_rate_measured_here_err=round(rate_ratio * d_err, 3))
         learned_extra = {"metropolis_link_updates_per_s_fp32_learned": world * 4 * V * 20 / t_l,
                          "esj_per_link_update_learned": rep["esj_learned"],
                          "esj_per_link_update_plain": rep["esj_plain_reference_proposal"],
@@ -534,7 +561,7 @@ def run_gpu(args):
                                              fp32_pipe=metro_fp32_pipe),
             "metropolis_link_updates_per_s_fp64": metro64_rate,
             "learned": learned_extra,
-            "eff_Q_samples_study": EFF_Q_STUDY,
+            "eff_Q_samples_study": eff_q_here,
             "ensemble_64_uneven": ens_extra,
             "metropolis_acceptance": acc_holder.get("a"),
             "plaq_after_flow": float(obs_last[0]),
