@@ -11,7 +11,8 @@ two spawned processes.
 
 Properties that hold at any size: gauge invariance (the reference's own
 check, latticeoperations.cpp:750-813), covariance under a one-site shift in
-time (which swaps the parities of every site), FP32 against FP64 over a flow,
+time (which swaps the parities of every site), the sign change of Q and q(t)
+under a reflection x -> -x, FP32 against FP64 over a flow,
 sweeps that compose, per-site densities that sum to the global observables,
 and unitarity after the flow."""
 import multiprocessing as mp
@@ -22,7 +23,7 @@ import numpy as np
 import pytest
 
 from conftest import ROOT, assert_obs_close, obs_errors, rel_err
-from test_oracle import gauge_transform
+from test_oracle import flip_charge, gauge_transform, reflect_x
 
 pytestmark = pytest.mark.gpu
 
@@ -127,6 +128,24 @@ def test_time_shift_covariance_full_size(g, start, prec):
     assert rel_err(b[[0, 2]], a[[0, 2]]) < TOL[prec]
     assert abs(b[1] - a[1]) < Q_TOL[prec]
     assert np.max(np.abs(b[3:] - np.roll(a[3:], 1))) < Q_TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_reflection_flips_the_charge_full_size(g, start, prec):
+    # x -> -x reverses the orientation: the plaquette and E stay, Q and q(t)
+    # change sign, at t = 0 and over 10 flow steps (the flow commutes with it)
+    obs = {}
+    for name, f in (("a", start), ("r", reflect_x(start, N))):
+        with g.Lattice(N, beta=6.2, precision=prec, flow_eps=0.01) as L:
+            L.set_links(f)
+            obs[name] = L.flow(10)
+    r, fa = obs["r"], flip_charge(obs["a"])
+    e = obs_errors(r[:, [0, 2]], fa[:, [0, 2]], scalars=("plaq", "energy"), slices=())
+    assert max(e.values()) < 10 * TOL[prec], e
+    assert np.max(np.abs(r[:, 1] - fa[:, 1])) < Q_TOL[prec]
+    assert np.max(np.abs(r[:, 3:] - fa[:, 3:])) < Q_TOL[prec]
+    print(prec, "reflection: plaq/E", e, "Q at t = 0 and after 10 steps", obs["a"][[0, -1], 1],
+          "max |dQ|", np.max(np.abs(r[:, 1] - fa[:, 1])))
 
 
 def test_fp32_flow_tracks_fp64_full_size(g, start):

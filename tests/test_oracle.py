@@ -132,6 +132,40 @@ def gauge_transform(L, W, N):
     return from_c(out)
 
 
+def reflect_x(L, N):
+    """The field reflected in x (x -> -x mod Nx): U'_mu(n) = U_mu(R n) for mu != 0
+    and U'_0(n) = U_0(R n - e_0)^+, the link from R n to R n - e_0 walked
+    backwards.  A reflection reverses the orientation: the plaquette and E stay,
+    Q and every q(t) change sign."""
+    Nx = N[0]
+    Lc = to_c(L).reshape((4,) + tuple(N[::-1]) + (3, 3))  # [mu, t, z, y, x, 3, 3]
+    out = Lc[:, :, :, :, (-np.arange(Nx)) % Nx].copy()
+    back = Lc[0][:, :, :, (-np.arange(Nx) - 1) % Nx]
+    out[0] = np.conj(np.swapaxes(back, -1, -2))
+    return from_c(out.reshape(4, -1, 3, 3))
+
+
+def flip_charge(obs):
+    """[plaq, topc, energy, topct[Nt]] with the charge and its slices negated."""
+    o = np.array(obs, np.float64, copy=True)
+    o[..., 1] *= -1
+    o[..., 3:] *= -1
+    return o
+
+
+def test_oracle_reflection_flips_the_charge(oracle):
+    # the parity symmetry Q -> -Q, and the flow commutes with the reflection
+    N = (4, 4, 4, 8)
+    L = oracle.haar_field(N, 31)
+    R = reflect_x(L, N)
+    assert rel_err(reflect_x(R, N), L) == 0.0
+    o, r = oracle.observables(N, L), oracle.observables(N, R)
+    assert abs(o[1]) > 1e-3
+    assert np.max(np.abs(r - flip_charge(o))) < 1e-12 * np.max(np.abs(o))
+    F = oracle.flow(N, L, 0.01, 3)
+    assert rel_err(oracle.flow(N, R, 0.01, 3), reflect_x(F, N)) < 1e-13
+
+
 def test_haar_field_is_special_unitary(oracle):
     L = oracle.haar_field((4, 4, 4, 4), 1234)
     M = to_c(L.reshape(-1, 18))
