@@ -54,7 +54,7 @@ def obs_errors(a, b, scalars=OBS_SCALARS, slices=("topct",)):
 
     a, b: one vector or rows of vectors laid out as the named scalars followed
     by equally long per-time-slice arrays ([plaq, topc, energy, topct[Nt]] by
-    default).  Each scalar is judged against its own value, each per-slice
+    default).  Each scalar is compared with its own value, each per-slice
     array against the largest |entry| of that array in the same row.
     Returns {name: max over rows}.
     """

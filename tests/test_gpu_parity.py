@@ -2,10 +2,10 @@
 reference.  Tolerances: FP64 <= 1e-12 relative, FP32 <= 1e-5 relative (the
 bars of the hot-path specification); accept decisions bit-identical.
 
-Observable vectors are judged one quantity at a time (conftest.obs_errors):
+Observable vectors are compared one quantity at a time (conftest.obs_errors):
 the plaquette, Q and the energy each against its own value, q(t) against the
 largest |q(t)| of its row.  Matrices (links, staples, forces, exponentials),
-whose entries are all of order one, are judged by the largest entry error
+whose entries are all of order one, are compared by the largest entry error
 against the largest entry (conftest.rel_err)."""
 import os
 
