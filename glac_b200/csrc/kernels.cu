@@ -64,7 +64,7 @@ __device__ __forceinline__ void flow_stage_body(const Geom &g, const LinkField<T
     if (s >= g.Vh) return;
     const int mu = plane >> 1, p = plane & 1;
     const Site n = site_from_ps(g, p, s);
-    M3<T> A = staple(in, g, n, p, mu);
+    M3<T> A = staple<T, false, true>(in, g, n, p, mu);
     const M3<T> U = in.load(mu, p, s);
     const AH8<T> Z = project_ah(mul(U, A));
     AH8<T> M;
@@ -133,14 +133,14 @@ __device__ __forceinline__ void flow_stage_site_body(const Geom &g, const LinkFi
                 M3<T> W;
                 if (nu > mu) {
                     const int s_nup = (n.lex + step_offset(g, n, nu, +1)) >> 1;
-                    const M3<T> t = mul_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
+                    const M3<T> t = flow_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
                     T *slot = my + 18 * kSiteBlock * tslot(mu, nu);
 #pragma unroll
                     for (int e = 0; e < 9; e++) {
                         slot[(2 * e) * kSiteBlock] = t.e[e].re;
                         slot[(2 * e + 1) * kSiteBlock] = t.e[e].im;
                     }
-                    W = mul_nd(t, in.load(nu, p, s));
+                    W = flow_nd(t, in.load(nu, p, s));
                 } else {
                     const T *slot = my + 18 * kSiteBlock * tslot(nu, mu);
                     M3<T> t;
@@ -149,15 +149,15 @@ __device__ __forceinline__ void flow_stage_site_body(const Geom &g, const LinkFi
                         t.e[e].re = slot[(2 * e) * kSiteBlock];
                         t.e[e].im = slot[(2 * e + 1) * kSiteBlock];
                     }
-                    W = mul_dd(t, in.load(nu, p, s));
+                    W = flow_dd(t, in.load(nu, p, s));
                 }
                 add_to(A, W);
                 plaq += retr_mul(in.load(mu, p, s), W);  // ReTr(U S_up)
                 asm volatile("" ::: "memory");
                 {
                     const int s_num = (n.lex + b_nu) >> 1, s_diag = (n.lex + f_mu + b_nu) >> 1;
-                    M3<T> t = mul_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
-                    const M3<T> S = mul(t, in.load(nu, q, s_num));
+                    M3<T> t = flow_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
+                    const M3<T> S = flow_nn(t, in.load(nu, q, s_num));
                     add_to(A, S);
                     sub_from(W, S);
                 }
@@ -171,7 +171,7 @@ __device__ __forceinline__ void flow_stage_site_body(const Geom &g, const LinkFi
             }
             if (nu > mu) {
                 const int s_nup = (n.lex + step_offset(g, n, nu, +1)) >> 1;
-                const M3<T> t = mul_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
+                const M3<T> t = flow_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
                 T *slot = my + 18 * kSiteBlock * tslot(mu, nu);
 #pragma unroll
                 for (int e = 0; e < 9; e++) {
@@ -191,7 +191,7 @@ __device__ __forceinline__ void flow_stage_site_body(const Geom &g, const LinkFi
             }
             {
                 const int s_num = (n.lex + b_nu) >> 1, s_diag = (n.lex + f_mu + b_nu) >> 1;
-                M3<T> t = mul_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
+                M3<T> t = flow_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
                 acc_mul(A, t, in.load(nu, q, s_num));
             }
         }
@@ -410,11 +410,11 @@ __device__ __forceinline__ void flow_stage0_meas_body(const Geom &g, const LinkF
         }
         if (!meas_takes(mu, nu)) {
             {
-                M3<T> t = mul_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
+                M3<T> t = flow_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
                 acc_mul_nd(A, t, in.load(nu, p, s));
             }
             {
-                M3<T> t = mul_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
+                M3<T> t = flow_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
                 acc_mul(A, t, in.load(nu, q, s_num));
             }
             continue;
@@ -422,15 +422,15 @@ __device__ __forceinline__ void flow_stage0_meas_body(const Geom &g, const LinkF
         // this thread's plane: the staple pieces separately, then W = S_up - S_low
         M3<T> W;
         {
-            M3<T> t = mul_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
-            W = mul_nd(t, in.load(nu, p, s));
+            M3<T> t = flow_nd(in.load(nu, q, s_mu), in.load(mu, q, s_nup));
+            W = flow_nd(t, in.load(nu, p, s));
         }
         add_to(A, W);
         plaq += retr_mul(in.load(mu, p, s), W);  // ReTr(U S_up), the plaquette of the plane at n
         asm volatile("" ::: "memory");
         {
-            M3<T> t = mul_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
-            M3<T> S = mul(t, in.load(nu, q, s_num));
+            M3<T> t = flow_dd(in.load(nu, p, s_diag), in.load(mu, q, s_num));
+            M3<T> S = flow_nn(t, in.load(nu, q, s_num));
             add_to(A, S);
             sub_from(W, S);
         }

@@ -15,7 +15,25 @@ namespace glac {
 // n has parity p; n +- nu and n + mu have parity 1-p, n + mu - nu has parity p.
 // UNROLL: the nu loop unrolled, which made the Metropolis sub-sweep 1-4 % faster
 // and the flow stage 2-6 % slower on B200 (the flow keeps the rolled loop).
-template <typename T, bool UNROLL = false>
+// SU(3) x SU(3) products of the FP32 flow kernels: the third row from the
+// first two (su3.cuh, 96 instead of 108 multiply-adds); FP64 keeps the full
+// product, the form the reference computes.
+template <typename T> __device__ __forceinline__ M3<T> flow_nd(const M3<T> &a, const M3<T> &b) {
+    if constexpr (sizeof(T) == 4) return mul_nd_su3(a, b);
+    else return mul_nd(a, b);
+}
+template <typename T> __device__ __forceinline__ M3<T> flow_dd(const M3<T> &a, const M3<T> &b) {
+    if constexpr (sizeof(T) == 4) return mul_dd_su3(a, b);
+    else return mul_dd(a, b);
+}
+template <typename T> __device__ __forceinline__ M3<T> flow_nn(const M3<T> &a, const M3<T> &b) {
+    if constexpr (sizeof(T) == 4) return mul_su3(a, b);
+    else return mul(a, b);
+}
+
+// RECON: the SU(3) products of each staple term by flow_nd / flow_dd (the flow
+// stage); the Metropolis kernels keep the full products.
+template <typename T, bool UNROLL = false, bool RECON = false>
 __device__ __forceinline__ M3<T> staple(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu) {
     M3<T> A;
     set_zero(A);
@@ -41,14 +59,14 @@ __device__ __forceinline__ M3<T> staple(const LinkField<T> &L, const Geom &g, co
         {
             M3<T> a = L.load(nu, q, s_mu);
             M3<T> b = L.load(mu, q, s_nup);
-            M3<T> t = mul_nd(a, b);
+            M3<T> t = RECON ? flow_nd(a, b) : mul_nd(a, b);
             M3<T> c = L.load(nu, p, n.lex >> 1);
             acc_mul_nd(A, t, c);
         }
         {
             M3<T> a = L.load(nu, p, s_diag);
             M3<T> b = L.load(mu, q, s_num);
-            M3<T> t = mul_dd(a, b);
+            M3<T> t = RECON ? flow_dd(a, b) : mul_dd(a, b);
             M3<T> c = L.load(nu, q, s_num);
             acc_mul(A, t, c);
         }
