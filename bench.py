@@ -48,19 +48,18 @@ WORKLOAD = "GLAC gradient flow 32^3x64, beta=6.2, eps=0.01, FP32 links + FP64 su
 # reads 4 links + writes 4 links per stage, force written (stage 0), read+written (1), read (2)
 STAGE_BYTES_FP32 = (8 * 72 + 4 * 32, 8 * 72 + 8 * 32, 8 * 72 + 4 * 32)
 STAGE_BYTES_FP64 = tuple(2 * b for b in STAGE_BYTES_FP32)
-NCU_TRAFFIC_STAGE0_FP32 = 636109568 + 837838592  # bytes, one ncu capture of the launch (uncapped variant)
 # stage 0 with the measurement's clover parts: + 12 slots x 32 B + 4 plaquette floats per site written
 STAGE0_MEAS_BYTES_FP32 = STAGE_BYTES_FP32[0] + 12 * 32 + 4 * 4
 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of that launch at
 # 32^3x64 (k_flow_stage0_meas_r128, profiles/flow_stage0_meas_fp32_32x32x32x64.md)
-NCU_TRAFFIC_STAGE0_MEAS_FP32 = 707364864 + 1667783168
+NCU_TRAFFIC_STAGE0_MEAS_FP32 = 707025920 + 1665065000
 # FP32 FLOP per site of that launch: (2 x FFMA + FADD + FMUL) thread instructions
-# counted by ncu = (2 x 14,914,945,024 + 1,472,200,704 + 1,400,897,536) / 2,097,152
-FLOPS_PER_SITE_STAGE0_MEAS_FP32 = 15594
-# FP32 floating-point operations per site of one stage-0 launch: 4 links x
-# (2 x FFMA + FADD + FMUL) thread instructions counted by ncu
-# (sm__sass_thread_inst_executed_op_{ffma,fadd,fmul}_pred_on) on the 32^3x64 launch
-FLOPS_PER_SITE_STAGE0_FP32 = 4 * (2 * 1547 + 59 + 95)
+# counted by ncu (sm__sass_thread_inst_executed_op_{ffma,fadd,fmul}_pred_on) on the
+# 32^3x64 launch = (2 x 13,178,503,168 + 1,472,200,704 + 1,627,389,952) / 2,097,152
+FLOPS_PER_SITE_STAGE0_MEAS_FP32 = 14046
+# the same count for the plain stage-0 launch (no measurement):
+# (2 x 12,071,206,912 + 494,927,872 + 1,098,907,648) / 2,097,152
+FLOPS_PER_SITE_STAGE0_FP32 = 12272
 SM_COUNT, FP32_LANES_PER_SM = 148, 128
 # The metric's third leg, effective Q samples/s of the learned FP32 sampler
 # against the plain FP64 GPU path at 32^3x64, beta = 6.2: a study of
@@ -355,17 +354,27 @@ def run_gpu(args):
 
     obs_buf = np.empty((args.steps + 1, 3 + DIMS[3]))
 
-    # clocks sampled from the warm-up through the timed region (nvidia-smi needs
-    # a moment to start, and the timed region lasts tens of milliseconds)
+    # clocks sampled under continuous load ending with the timed region: once
+    # nvidia-smi reports (it takes a moment to start), about a second of measured
+    # flow steps, then the warm-up and the timed steps (the timed region itself
+    # lasts tens of milliseconds, a fraction of the 100 ms sampling interval)
     clk = ClockSampler(local)
     clk.start()
-    time.sleep(0.5)
+    t_w = time.perf_counter()
+    while not clk.lines and time.perf_counter() - t_w < 5.0:
+        time.sleep(0.05)
+    clk.lines.clear()
+    t_w = time.perf_counter()
+    while time.perf_counter() - t_w < 1.0:
+        L.flow(10, measure=True)
+        L.sync()
     L.flow(args.warmup, measure=True)
     n0 = L.launch_count
     # timed: K RK3 steps, each followed by the observable measurement (device
     # buffer), all K+1 observable vectors copied back at the end
     t_main = timed(lambda: L.flow(args.steps, out=obs_buf), 1)
     clocks = clk.stop()
+    clocks["window"] = "continuous load: ~1 s of measured flow steps, the warm-up and the timed steps"
     launches = L.launch_count - n0
     value = world * V * args.steps / t_main
 
