@@ -99,16 +99,58 @@ def load_peaks():
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and clock-event reasons of one GPU, sampled in a thread while the
+    GPU works: by NVML queries every 2 ms (read-only: current and maximum SM
+    clock, current clock-event reasons), or by `nvidia-smi -lms 100` where NVML
+    is unavailable.  stop(window) summarises the samples taken inside the
+    perf_counter window (t0, t1) when there are at least three, else all."""
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap", "hw_power_brake_slowdown")
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, period_s: float = 0.002):
         self.dev = device_index
+        self.period = period_s
+        self.samples = []  # (perf_counter, sm MHz, set of reasons)
+        self.smax = None
         self.proc = None
-        self.lines = []
+        self.nvml = None
+        self.stop_flag = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        n = pynvml.nvmlDeviceGetCount()
+        uuid = None
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+        except Exception:
+            uuid = None
+        for i in range(n):
+            h = pynvml.nvmlDeviceGetHandleByIndex(i)
+            u = pynvml.nvmlDeviceGetUUID(h)
+            u = u.decode() if isinstance(u, bytes) else u
+            if uuid and u.replace("GPU-", "") == uuid.replace("GPU-", ""):
+                return pynvml, h
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev if self.dev < n else 0)
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap,
+                    "hw_power_brake_slowdown": nv.nvmlClocksEventReasonHwPowerBrakeSlowdown}
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.nvml = (nv, h, bits)
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -118,34 +160,56 @@ class ClockSampler:
         except FileNotFoundError:
             self.proc = None
 
+    def _poll(self):
+        nv, h, bits = self.nvml
+        while not self.stop_flag.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:
+                break
+            self.samples.append((time.perf_counter(), sm, {k for k, b in bits.items() if r & b}))
+            time.sleep(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
+            parts = [p.strip() for p in line.strip().split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
+                sm = float(parts[1])
+                self.smax = float(parts[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+            rs = {nm for nm, v in zip(self.NAMES[:4], parts[5:9]) if v.lower().startswith("active")}
+            self.samples.append((time.perf_counter(), sm, rs))
+
+    def stop(self, window=None):
+        if self.nvml:
+            self.stop_flag.set()
+            self.t.join(timeout=5)
+            how = "NVML every 2 ms"
+        elif self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            how = "nvidia-smi every 100 ms"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        sel = self.samples
+        if window is not None:
+            inside = [x for x in self.samples if window[0] <= x[0] <= window[1]]
+            if len(inside) >= 3:
+                sel = inside
+        sm = [x[1] for x in sel]
+        reasons = set().union(*[x[2] for x in sel]) if sel else set()
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                "sm_mhz_min": min(sm) if sm else None, "reasons": sorted(reasons), "samples": len(sm),
+                "sampled_by": how,
+                "window": ("all samples" if window is None else
+                           "timed region" if sel is not self.samples else "all samples (under 3 in the timed region)")}
 
 
 # ---------------------------------------------------------------------------
@@ -354,32 +418,32 @@ def run_gpu(args):
 
     obs_buf = np.empty((args.steps + 1, 3 + DIMS[3]))
 
-    # clocks sampled under continuous load ending with the timed region: once
-    # nvidia-smi reports (it takes a moment to start), about a second of measured
-    # flow steps, then the warm-up and the timed steps (the timed region itself
-    # lasts tens of milliseconds, a fraction of the 100 ms sampling interval)
+    # clocks sampled from the warm-up through the timed region; the summary
+    # takes the samples inside the timed region (NVML polls every 2 ms)
     clk = ClockSampler(local)
     clk.start()
-    t_w = time.perf_counter()
-    while not clk.lines and time.perf_counter() - t_w < 5.0:
-        time.sleep(0.05)
-    clk.lines.clear()
-    t_w = time.perf_counter()
-    while time.perf_counter() - t_w < 1.0:
-        L.flow(10, measure=True)
-        L.sync()
+    time.sleep(0.5)
     L.flow(args.warmup, measure=True)
     n0 = L.launch_count
     # timed: K RK3 steps, each followed by the observable measurement (device
     # buffer), all K+1 observable vectors copied back at the end
+    tw0 = time.perf_counter()
     t_main = timed(lambda: L.flow(args.steps, out=obs_buf), 1)
-    clocks = clk.stop()
-    clocks["window"] = "continuous load: ~1 s of measured flow steps, the warm-up and the timed steps"
+    clocks = clk.stop(window=(tw0, time.perf_counter()))
     launches = L.launch_count - n0
     value = world * V * args.steps / t_main
 
     t_noobs = timed(lambda: L.flow(args.steps, measure=False), 1)
     rate_noobs = world * V * args.steps / t_noobs
+
+    # sustained: measured flow steps over about two seconds of continuous load
+    # (the GPU reaches its power cap within that time), clocks sampled meanwhile
+    clk_s = ClockSampler(local)
+    clk_s.start()
+    n_sus = max(100, int(2.0 / (t_main / args.steps)))
+    t_sus = timed(lambda: L.flow(n_sus, measure=True), 1)
+    sustained = {"site_steps_per_s": world * V * n_sus / t_sus, "steps": n_sus, "seconds": t_sus,
+                 "clocks": clk_s.stop()}
 
     # roofline of the flow-stage kernel: CUDA events around each stage launch on
     # the lattice's stream, averaged over reps RK3 steps
@@ -563,6 +627,7 @@ def run_gpu(args):
         "clocks": clocks,
         "extra": {
             "flow_site_steps_per_s_no_obs": rate_noobs,
+            "flow_sustained": sustained,
             "flow_site_steps_per_s_fp64_with_obs": rate64,
             "metropolis_link_updates_per_s_fp32": metro_rate,
             "metropolis_roofline_fp32": dict(metro_roofline, peak=hbm_peak,
