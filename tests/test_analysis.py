@@ -47,3 +47,46 @@ def test_replica_gamma_method_on_ar1():
     assert 0.2 * r.tau_error < je < 5 * r.tau_error
     # one replica: the single-chain method
     assert gamma_method_replicas(chains[:1]).tau_int == gamma_method(chains[0]).tau_int
+
+
+def _study_runs(samplers, replicas, n_meas, meas_every=100, seed=0):
+    """Synthetic chains in the layout glac_b200.studies.target_run writes: Q is
+    an AR(1) series with per-measurement correlation rho (the same stationary
+    variance for every sampler), plaquette and E are white noise."""
+    chains = []
+    for si, (name, rho, sweep_s) in enumerate(samplers):
+        for r in range(replicas):
+            q = ar1(n_meas, rho, seed=seed + 1000 * si + r) * np.sqrt(1 - rho * rho) * 6.0
+            g = np.random.default_rng(seed + 7 + 1000 * si + r)
+            chains.append(dict(sampler=name, replica=r, meas_every=meas_every, sweeps=n_meas * meas_every,
+                               wall_s=n_meas * meas_every * sweep_s, acceptance=0.2, Q=q.tolist(),
+                               plaq=(0.61 + 1e-4 * g.standard_normal(n_meas)).tolist(),
+                               E=(-2.0 + 1e-3 * g.standard_normal(n_meas)).tolist()))
+    return [dict(config={"synthetic": True}, chains=chains)]
+
+
+def test_q_diffusion_estimator_on_known_chains():
+    # Two samplers of known tau_int,Q and cost: "plain_fp64" decorrelates over
+    # 3000 sweeps at 9.6 ms a sweep, "learned_fp32" over 1000 sweeps at 3.9 ms.
+    # For AR(1), <(Q_{i+k} - Q_i)^2> = 2 var (1 - rho^k) exactly, so the
+    # diffusion ratio at lag k has a known expectation, which lies below the
+    # ratio of effective samples per second (1 - rho^k is concave in the
+    # decorrelation rate): the estimator can only understate the faster sampler.
+    from glac_b200.studies import target_combine
+    every = 100
+    rho_a, rho_b = np.exp(-every / 3000.0), np.exp(-every / 1000.0)
+    res = target_combine(_study_runs([("plain_fp64", rho_a, 9.6e-3), ("learned_fp32", rho_b, 3.9e-3)],
+                                     replicas=48, n_meas=600))["samplers"]
+    tau = lambda rho: (1 + rho) / (2 * (1 - rho))
+    true_ratio = (tau(rho_a) * 9.6e-3) / (tau(rho_b) * 3.9e-3)
+    for lag in (200, 500, 1000):
+        k = lag // every
+        expect = ((1 - rho_b ** k) / 3.9e-3) / ((1 - rho_a ** k) / 9.6e-3)
+        got = res["learned_fp32"][f"eff_Q_ratio_vs_plain_fp64_diffusion_{lag}"]
+        err = res["learned_fp32"][f"eff_Q_ratio_vs_plain_fp64_diffusion_{lag}_err"]
+        assert expect < true_ratio
+        assert abs(got - expect) < 4 * err and err < 0.1 * expect, (lag, got, expect, err)
+    # the replica Gamma method finds tau_int,Q of each sampler (in sweeps)
+    for name, rho in (("plain_fp64", rho_a), ("learned_fp32", rho_b)):
+        assert abs(res[name]["tau_Q"] - tau(rho) * every) < 4 * res[name]["tau_Q_err"]
+    assert res["plain_fp64"]["eff_Q_ratio_vs_plain_fp64"] == 1.0
