@@ -402,7 +402,7 @@ def run_gpu(args):
     L.hot_start(20261203)
     L.metropolis(5)
     L.reunitarize()
-    tuned = L.autotune(3)
+    tuned = L.autotune(8)  # launch variants timed over 8 repetitions each (flow: measured steps)
     acc_holder = {}
     t_metro = timed(lambda: acc_holder.setdefault("a", L.metropolis(1)), 20)
     L.metropolis(THERM_SWEEPS - 25)

@@ -710,8 +710,12 @@ glac_status glac_autotune(glac_ctx *c, int reps, double *report) {
                 for (int pass = 0; pass < 2; pass++) {  // pass 0 warms up
                     ck(cudaEventRecord(e0, c->stream), "event");
                     for (int r = 0; r < reps; r++) {
-                        if (fam == FAM_FLOW) flow_step(c);
-                        else if (fam == FAM_METRO) {
+                        // flows measure after every step where the measurement runs
+                        // inside the stages, so the flow family is timed on such steps
+                        if (fam == FAM_FLOW) {
+                            if (fused_measure_usable(c)) flow_step(c, nullptr, c->obs_dev);
+                            else flow_step(c);
+                        } else if (fam == FAM_METRO) {
                             for (int k = 0; k < 8; k++) {
                                 if (fp32)
                                     launch_metropolis(c->g, f32(c, c->cur), k >> 1, k & 1, c->d.beta, c->d.su3_eps,
