@@ -9,12 +9,6 @@
 
 namespace glac {
 
-// Staple A_mu(n) (GLAC/actions/wilsongaugeaction.cpp:29-53, and the same sum in
-// getActionDerivative :55-86):
-//   sum_{nu != mu}  U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+  +  U_nu(n+mu-nu)^+ U_mu(n-nu)^+ U_nu(n-nu)
-// n has parity p; n +- nu and n + mu have parity 1-p, n + mu - nu has parity p.
-// UNROLL: the nu loop unrolled, which made the Metropolis sub-sweep 1-4 % faster
-// and the flow stage 2-6 % slower on B200 (the flow keeps the rolled loop).
 // SU(3) x SU(3) products of the FP32 flow kernels: the third row from the
 // first two (su3.cuh, 96 instead of 108 multiply-adds); FP64 keeps the full
 // product, the form the reference computes.
@@ -31,7 +25,13 @@ template <typename T> __device__ __forceinline__ M3<T> flow_nn(const M3<T> &a, c
     else return mul(a, b);
 }
 
-// RECON: the SU(3) products of each staple term by flow_nd / flow_dd (the flow
+// Staple A_mu(n) (GLAC/actions/wilsongaugeaction.cpp:29-53, and the same sum in
+// getActionDerivative :55-86):
+//   sum_{nu != mu}  U_nu(n+mu) U_mu(n+nu)^+ U_nu(n)^+  +  U_nu(n+mu-nu)^+ U_mu(n-nu)^+ U_nu(n-nu)
+// n has parity p; n +- nu and n + mu have parity 1-p, n + mu - nu has parity p.
+// UNROLL: the nu loop unrolled, which made the Metropolis sub-sweep 1-4 % faster
+// and the flow stage 2-6 % slower on B200 (the flow keeps the rolled loop).
+// RECON: each staple term's first product by flow_nd / flow_dd (the flow
 // stage); the Metropolis kernels keep the full products.
 template <typename T, bool UNROLL = false, bool RECON = false>
 __device__ __forceinline__ M3<T> staple(const LinkField<T> &L, const Geom &g, const Site &n, int p, int mu) {
